@@ -1,0 +1,193 @@
+// Common infrastructure of the B200 partitioner: graph type widths, status
+// codes and exceptions, the per-context stream-ordered allocator and small
+// device helpers shared by every stage.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "../../include/gpart_b200.h"
+
+namespace gp {
+
+using u64 = std::uint64_t;
+using u32 = std::uint32_t;
+using i64 = std::int64_t;
+using i32 = std::int32_t;
+
+// The reference's two graph widths (include/graph_types.hpp:7-17):
+// "standard" = int32 offsets + uint32 weights, "big" = int64 offsets +
+// uint64 weights.  Vertex ids are int32 in both.
+struct Std { using O = i32; using W = u32; static constexpr const char* name = "standard"; };
+struct Big { using O = i64; using W = u64; static constexpr const char* name = "big"; };
+
+// Errors carry the C-ABI status.  The classes mirror the reference's
+// exception classes: invalid_argument -> GP_EINVAL, runtime_error ->
+// GP_ERUNTIME, overflow_error -> GP_EOVERFLOW.
+struct Error : std::runtime_error {
+    gp_status status;
+    Error(gp_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+};
+[[noreturn]] inline void fail(gp_status s, const std::string& what) { throw Error(s, what); }
+
+#define GP_CUDA(call)                                                              \
+    do {                                                                           \
+        const cudaError_t e__ = (call);                                            \
+        if (e__ != cudaSuccess)                                                    \
+            ::gp::fail(e__ == cudaErrorMemoryAllocation ? GP_ENOMEM : GP_ECUDA,    \
+                       std::string("CUDA failure at ") + __FILE__ + ":" +          \
+                           std::to_string(__LINE__) + " " + #call + ": " +         \
+                           cudaGetErrorString(e__));                               \
+    } while (0)
+
+#define GP_LAUNCH() GP_CUDA(cudaGetLastError())
+
+// Device error word bits (set by kernels, read at host sync points).
+enum DeviceError : u32 {
+    kErrNone = 0,
+    kErrTimeout = 1u << 0,        // a bounded wait gave up
+    kErrCapacity = 1u << 1,       // SCLP cluster above its cap
+    kErrSplit = 1u << 2,          // spectral split cannot satisfy capacity
+    kErrBalance = 1u << 3,        // initial partition above capacity
+    kErrCutUnderflow = 1u << 4,   // incremental cut underflow
+    kErrOddCut = 1u << 5,         // directed cut odd (asymmetric input)
+    kErrTableFull = 1u << 6,      // hash table overflow (sizing bug)
+    kErrBadInput = 1u << 7,       // input validation failure
+};
+
+// ---------------------------------------------------------------------------
+// Stream-ordered device allocation from a per-context memory pool that keeps
+// freed blocks cached (release threshold = UINT64_MAX), so repeated
+// partitions in one context allocate without touching the driver.
+// ---------------------------------------------------------------------------
+struct Device {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    int sms = 148;
+    u32* err = nullptr;         // device error word
+    void* pinned = nullptr;     // small pinned host staging area
+    static constexpr size_t kPinnedBytes = 1 << 16;
+
+    void* alloc(size_t bytes) {
+        if (bytes == 0) return nullptr;
+        void* p = nullptr;
+        GP_CUDA(cudaMallocFromPoolAsync(&p, (bytes + 255) & ~size_t{255}, pool, stream));
+        return p;
+    }
+    void release(void* p) {
+        if (p) cudaFreeAsync(p, stream);
+    }
+    void sync() { GP_CUDA(cudaStreamSynchronize(stream)); }
+    // Read a device error word; throws on any set bit.
+    void check_errors();
+};
+
+template <typename T>
+class Buf {
+public:
+    Buf() = default;
+    Buf(Device& d, size_t count) : dev_(&d), count_(count) {
+        ptr_ = static_cast<T*>(d.alloc(count * sizeof(T)));
+    }
+    ~Buf() { reset(); }
+    Buf(Buf&& o) noexcept : dev_(o.dev_), ptr_(o.ptr_), count_(o.count_) { o.ptr_ = nullptr; o.count_ = 0; }
+    Buf& operator=(Buf&& o) noexcept {
+        if (this != &o) { reset(); dev_ = o.dev_; ptr_ = o.ptr_; count_ = o.count_; o.ptr_ = nullptr; o.count_ = 0; }
+        return *this;
+    }
+    Buf(const Buf&) = delete;
+    Buf& operator=(const Buf&) = delete;
+    void reset() { if (ptr_ && dev_) dev_->release(ptr_); ptr_ = nullptr; count_ = 0; }
+    // Grow without preserving contents.
+    void ensure(Device& d, size_t count) {
+        if (count <= count_ && ptr_) return;
+        reset();
+        dev_ = &d;
+        count_ = count;
+        ptr_ = static_cast<T*>(d.alloc(count * sizeof(T)));
+    }
+    T* get() const { return ptr_; }
+    size_t size() const { return count_; }
+    void zero(Device& d) { if (count_) GP_CUDA(cudaMemsetAsync(ptr_, 0, count_ * sizeof(T), d.stream)); }
+    void fill_bytes(Device& d, int byte) { if (count_) GP_CUDA(cudaMemsetAsync(ptr_, byte, count_ * sizeof(T), d.stream)); }
+    void swap(Buf& o) { std::swap(dev_, o.dev_); std::swap(ptr_, o.ptr_); std::swap(count_, o.count_); }
+
+private:
+    Device* dev_ = nullptr;
+    T* ptr_ = nullptr;
+    size_t count_ = 0;
+};
+
+template <typename T>
+void to_host(Device& d, T* host, const T* dev, size_t count) {
+    if (count) GP_CUDA(cudaMemcpyAsync(host, dev, count * sizeof(T), cudaMemcpyDeviceToHost, d.stream));
+}
+template <typename T>
+void to_device(Device& d, T* dev, const T* host, size_t count) {
+    if (count) GP_CUDA(cudaMemcpyAsync(dev, host, count * sizeof(T), cudaMemcpyHostToDevice, d.stream));
+}
+// Synchronously fetch a few scalars through the pinned staging area.
+template <typename T>
+void fetch(Device& d, T* host, const T* dev, size_t count) {
+    static_assert(std::is_trivially_copyable_v<T>);
+    if (!count) return;
+    const size_t bytes = count * sizeof(T);
+    if (bytes > Device::kPinnedBytes) { to_host(d, host, dev, count); d.sync(); return; }
+    GP_CUDA(cudaMemcpyAsync(d.pinned, dev, bytes, cudaMemcpyDeviceToHost, d.stream));
+    d.sync();
+    std::memcpy(host, d.pinned, bytes);
+}
+
+inline int blocks_for(i64 items, int per_block) {
+    const i64 b = (items + per_block - 1) / per_block;
+    return static_cast<int>(b < 1 ? 1 : b);
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+// The reference's 32-bit mixer (src/coarsen.cu:112-118, refine.cu:38-44,
+// initial_partition_gpu.cu:36-39).
+__host__ __device__ __forceinline__ u32 mix32(u32 x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    return x ^ (x >> 16);
+}
+
+template <typename W>
+__device__ __forceinline__ W weight_at(const W* w, i64 i) { return w ? w[i] : W(1); }
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ void atomic_add_w(u32* p, u32 v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_w(u64* p, u64 v) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ u64 atomic_add_u64(u64* p, u64 v) {
+    return atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ u64 atomic_max_u64(u64* p, u64 v) {
+    return atomicMax(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ u64 atomic_cas_u64(u64* p, u64 c, u64 v) {
+    return atomicCAS(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(c),
+                     static_cast<unsigned long long>(v));
+}
+
+__device__ __forceinline__ void set_error(u32* err, u32 bit) { atomicOr(err, bit); }
+
+}  // namespace gp

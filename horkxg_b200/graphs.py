@@ -1,0 +1,133 @@
+"""Synthetic workloads in the partitioner's on-disk input format.
+
+Each generator writes native-endian int64 ``indptr``/``indices`` files (the
+format read by the reference's ``gpart_partition_*`` drivers, ``src/graph.cpp``
+lines 47-122) and caches them by parameters, so both the B200 build and the
+reference binary read byte-identical inputs.  Generation is done by the
+multithreaded C++ code in ``csrc/gen.cpp``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = _HERE / "libgpgen.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} is missing; run __graft_entry__.build()")
+        lib = ctypes.CDLL(str(path))
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        lib.gp_gen_last_error.restype = ctypes.c_char_p
+        lib.gp_gen_grid2d.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_char_p, ctypes.c_char_p, i64p, i64p]
+        lib.gp_gen_grid3d.argtypes = [ctypes.c_int64] * 3 + [ctypes.c_char_p, ctypes.c_char_p, i64p, i64p]
+        lib.gp_gen_rmat.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p,
+                                    i64p, i64p]
+        lib.gp_gen_rgg.argtypes = [ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, ctypes.c_char_p,
+                                   ctypes.c_char_p, i64p, i64p]
+        _LIB = lib
+    return _LIB
+
+
+def cache_dir() -> Path:
+    root = Path(os.environ.get("GP_GRAPH_CACHE", "/tmp/gp_graphs"))
+    root.mkdir(parents=True, exist_ok=True)
+    return root
+
+
+def _run(name: str, fn, *args) -> tuple[Path, Path]:
+    root = cache_dir() / name
+    root.mkdir(parents=True, exist_ok=True)
+    indptr, indices = root / "indptr.bin", root / "indices.bin"
+    if indptr.exists() and indices.exists():
+        return indptr, indices
+    n, m = ctypes.c_int64(), ctypes.c_int64()
+    rc = fn(*args, str(indptr).encode(), str(indices).encode(), ctypes.byref(n), ctypes.byref(m))
+    if rc != 0:
+        raise RuntimeError(_lib().gp_gen_last_error().decode())
+    return indptr, indices
+
+
+def grid2d(nx: int, ny: int) -> tuple[Path, Path]:
+    return _run(f"grid2d_{nx}x{ny}", _lib().gp_gen_grid2d, nx, ny)
+
+
+def grid3d(nx: int, ny: int, nz: int) -> tuple[Path, Path]:
+    return _run(f"grid3d_{nx}x{ny}x{nz}", _lib().gp_gen_grid3d, nx, ny, nz)
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+         seed: int = 1) -> tuple[Path, Path]:
+    name = f"rmat_s{scale}_ef{edge_factor}_{a}_{b}_{c}_seed{seed}"
+    return _run(name, _lib().gp_gen_rmat, scale, edge_factor, a, b, c, seed)
+
+
+def rgg(n: int, mean_degree: float = 10.0, seed: int = 7) -> tuple[Path, Path]:
+    radius = math.sqrt(mean_degree / (math.pi * n))
+    return _run(f"rgg_n{n}_deg{mean_degree}_seed{seed}", _lib().gp_gen_rgg, n, radius, seed)
+
+
+def write_csr(name: str, offsets, indices) -> tuple[Path, Path]:
+    """Write an explicit int64 CSR (used for small hand-made fixtures)."""
+    root = cache_dir() / name
+    root.mkdir(parents=True, exist_ok=True)
+    indptr, idx = root / "indptr.bin", root / "indices.bin"
+    np.asarray(offsets, dtype=np.int64).tofile(indptr)
+    np.asarray(indices, dtype=np.int64).tofile(idx)
+    return indptr, idx
+
+
+def load(indptr: Path, indices: Path) -> tuple[np.ndarray, np.ndarray]:
+    """Memory-map an int64 CSR pair."""
+    off = np.fromfile(indptr, dtype=np.int64)
+    idx = np.memmap(indices, dtype=np.int64, mode="r") if os.path.getsize(indices) else np.zeros(0, np.int64)
+    return off, idx
+
+
+def by_name(name: str) -> tuple[Path, Path]:
+    """Named workloads shared by tests, the golden-vector script and bench.py."""
+    table = {
+        "grid2d_256": lambda: grid2d(256, 256),
+        "grid2d_64": lambda: grid2d(64, 64),
+        "grid3d_24": lambda: grid3d(24, 24, 24),
+        "grid3d_320": lambda: grid3d(320, 320, 320),
+        "rmat12": lambda: rmat(12),
+        "rmat14": lambda: rmat(14),
+        "rmat16": lambda: rmat(16),
+        "rmat22": lambda: rmat(22),
+        "rmat24": lambda: rmat(24),
+        "rmat26": lambda: rmat(26),
+        "rgg_20k": lambda: rgg(20000),
+        "cycle_hub_4096": cycle_hub,
+    }
+    return table[name]()
+
+
+def cycle_hub(n: int = 4096, spokes: int = 512) -> tuple[Path, Path]:
+    """4096-cycle plus a 512-spoke hub at vertex 0 with a hub self loop: the
+    unit-weight form of the reference fixture in tests/test_uncoarsen.cu:233-285."""
+    rows = [[] for _ in range(n)]
+    for v in range(n):
+        rows[v].append((v + 1) % n)
+        rows[(v + 1) % n].append(v)
+    for v in range(1, spokes + 1):
+        rows[0].append(v)
+        rows[v].append(0)
+    rows[0].append(0)
+    offsets = [0]
+    indices = []
+    for r in rows:
+        r.sort()
+        indices.extend(r)
+        offsets.append(len(indices))
+    return write_csr(f"cycle_hub_{n}_{spokes}", offsets, indices)

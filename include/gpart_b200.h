@@ -1,0 +1,181 @@
+/*
+ * gpart_b200.h - C ABI of the B200-native multilevel k-way graph partitioner.
+ *
+ * The library replaces the partition path behind the reference's
+ * gpart_partition_standard / gpart_partition_big drivers
+ * (app/partition_main.cu:20-142): SCLP coarsening, recursive spectral
+ * bisection and incremental bucketed refinement, from CSR to int32 labels.
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or
+ * torch types.  A context owns one CUDA stream and a memory pool on one GPU;
+ * it is not thread-safe (one context per host thread, as the reference's
+ * scratch pool is thread_local, include/detail/scratch_pool.hpp:35).
+ *
+ * Status codes follow the reference's exception classes:
+ *   GP_EINVAL    <- std::invalid_argument (bad input, infeasible capacity)
+ *   GP_ERUNTIME  <- std::runtime_error   (spectral split infeasible, SCLP cap
+ *                                         exceeded, postconditions)
+ *   GP_EOVERFLOW <- std::overflow_error  (weight ranges)
+ * plus GP_ECUDA / GP_ENOMEM / GP_ETIMEOUT for device failures.
+ */
+#ifndef GPART_B200_H
+#define GPART_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gp_status {
+    GP_OK = 0,
+    GP_EINVAL = 1,
+    GP_ERUNTIME = 2,
+    GP_EOVERFLOW = 3,
+    GP_ECUDA = 4,
+    GP_ETIMEOUT = 5,
+    GP_ENOMEM = 6
+} gp_status;
+
+/* Graph widths: the reference's StandardTypes / BigTypes
+ * (include/graph_types.hpp:7-17). */
+enum { GP_WIDTH_STANDARD = 0, GP_WIDTH_BIG = 1 };
+/* Where the arrays of a gp_graph live. */
+enum { GP_MEMORY_HOST = 0, GP_MEMORY_DEVICE = 1 };
+
+/* A symmetric CSR graph.  With index64 = 0 the arrays use the width's types:
+ * offsets int32 (standard) / int64 (big), neighbours int32, weights
+ * uint32 / uint64.  With index64 = 1 offsets and neighbours are the int64
+ * arrays of the reference's input files (src/graph.cpp:47-122); the library
+ * narrows and validates them on the GPU with the reference's rules and
+ * messages.  NULL weights mean unit weights (the reference's file input always
+ * has unit weights, src/graph.cpp:117-118). */
+typedef struct gp_graph {
+    int64_t n;
+    int64_t m;
+    int32_t width;
+    int32_t memory;
+    int32_t index64;
+    int32_t reserved;
+    const void* offsets;
+    const void* neighbors;
+    const void* edge_weights;
+    const void* vertex_weights;
+} gp_graph;
+
+/* Partition options; gp_options_default() gives the production values of
+ * app/partition_main.cu:37-82. */
+typedef struct gp_options {
+    int32_t parts;               /* 2..32 */
+    int32_t cluster_size_factor; /* <= 0: max(64, ceil(512/parts)) */
+    double imbalance;            /* >= 1.0, default 1.03 */
+    uint32_t seed;
+    int32_t verify;              /* strict checks, the reference's --verify */
+    int32_t deterministic;       /* (gain, vertex id) ranking inside rebalance buckets */
+    int32_t pack_isolated;       /* default 1 */
+    int32_t max_levels;          /* default 24 */
+    int32_t max_rounds;          /* refinement phases per level, default 32 */
+    double stop_ratio;           /* default 0.90 */
+    double growth_ratio;         /* refine a level when n >= ratio * last refined n; 2.0 */
+    int32_t log;                 /* print the reference's key=value lines to stdout */
+    int32_t reserved;
+} gp_options;
+
+typedef struct gp_report {
+    int64_t n, m;
+    uint64_t cut;                 /* final undirected cut (final_edge_cut=) */
+    uint64_t capacity;            /* floor(ratio * W / k) */
+    uint64_t total_edge_weight;   /* undirected */
+    uint64_t part_weights[32];
+    int32_t levels;               /* hierarchy levels incl. the input */
+    int32_t reserved;
+    int64_t coarsest_n;
+    uint64_t initial_cut;         /* cut of the spectral partition on the coarsest level */
+    double coarsen_seconds;
+    double initial_seconds;
+    double uncoarsen_seconds;
+    double free_seconds;
+    double algorithm_seconds;     /* the reference's algorithm_total_seconds scope */
+    double prepare_seconds;       /* upload + narrowing + validation (outside the algorithm scope) */
+} gp_report;
+
+typedef struct gp_refine_stats {
+    int32_t rounds;
+    uint64_t proposals, accepted, initial_cut, final_cut, final_max_part_weight;
+    int32_t admission_iterations, admission_fallbacks;
+} gp_refine_stats;
+
+typedef struct gp_ctx gp_ctx;
+typedef struct gp_hierarchy gp_hierarchy;
+
+void gp_options_default(gp_options* options);
+
+/* Context on CUDA device `device`. */
+gp_status gp_ctx_create(int device, gp_ctx** out);
+void gp_ctx_destroy(gp_ctx* ctx);
+/* Message of the last failure on this context ("" if none). */
+const char* gp_ctx_error(const gp_ctx* ctx);
+
+/* include/partition_capacity.hpp:12-23 (host only). */
+gp_status gp_partition_capacity(uint64_t total, int parts, double ratio, uint64_t* out);
+
+/* Full pipeline (replaces app/partition_main.cu:59-96: coarsen,
+ * initial_partition_gpu, uncoarsen).  labels has n int32 entries, in host
+ * memory when graph->memory is HOST, else in device memory.  The report's
+ * algorithm_seconds covers the reference's algorithm_total_seconds scope:
+ * from the uploaded, validated graph to device labels with scratch released. */
+gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* options,
+                       int32_t* labels, gp_report* report);
+
+/* One SCLP aggregation (replaces gpart::aggregate, include/coarsen.hpp:88-92;
+ * src/coarsen.cu:1661-1671).  map: n int32 (host).  cluster_size_factor and
+ * pack_isolated are used as given. */
+gp_status gp_aggregate(gp_ctx* ctx, const gp_graph* graph, int parts, uint32_t seed, int level,
+                       int cluster_size_factor, int pack_isolated, int32_t* map,
+                       int64_t* coarse_n, uint64_t* cluster_cap);
+
+/* Contraction (replaces gpart::contract, include/coarsen.hpp:94-97;
+ * src/coarsen.cu:1826-1831).  Host outputs: offsets (coarse_n+1), neighbours
+ * and edge weights sized for at least graph->m entries, vertex weights
+ * (coarse_n); rows come out sorted by target. */
+gp_status gp_contract(gp_ctx* ctx, const gp_graph* graph, const int32_t* map, int64_t coarse_n,
+                      int64_t* offsets, int32_t* neighbors, uint64_t* edge_weights,
+                      uint64_t* vertex_weights, int64_t* coarse_m);
+
+/* Coarsening to a host hierarchy (replaces gpart::coarsen,
+ * include/coarsen.hpp:99-101; the export of app/coarsen_main.cu:13-79). */
+gp_status gp_coarsen(gp_ctx* ctx, const gp_graph* graph, const gp_options* options,
+                     gp_hierarchy** out);
+int32_t gp_hierarchy_levels(const gp_hierarchy* h);
+/* Copies level `level`; any output pointer may be NULL (then only sizes). */
+gp_status gp_hierarchy_level(const gp_hierarchy* h, int level, int64_t* n, int64_t* m,
+                             int64_t* offsets, int32_t* neighbors, uint64_t* edge_weights,
+                             uint64_t* vertex_weights, int32_t* map_to_next);
+/* The reference's write_hierarchy layout (include/hierarchy.hpp:42-126). */
+gp_status gp_hierarchy_write(const gp_hierarchy* h, const char* path);
+void gp_hierarchy_free(gp_hierarchy* h);
+
+/* Spectral initial partition (replaces gpart::initial_partition_gpu,
+ * include/initial_partition.hpp:9-12).  labels: n int32 (host). */
+gp_status gp_initial_partition(gp_ctx* ctx, const gp_graph* graph, int parts, double ratio,
+                               uint32_t seed, int32_t* labels);
+
+/* FP32 diffusion of one bisection task (src/initial_partition_gpu.cu:81-142):
+ * vertices with labels[v] == group, seed ^ group, `steps` steps; x: n floats
+ * (host), 0 outside the group. */
+gp_status gp_diffusion(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int group,
+                       uint32_t seed, int steps, float* x);
+
+/* Incremental bucketed refinement (replaces gpart::refine_partition,
+ * include/refine.hpp:57-61).  labels: n int32 (host), refined in place. */
+gp_status gp_refine(gp_ctx* ctx, const gp_graph* graph, int32_t* labels, int parts, double ratio,
+                    int max_rounds, int deterministic, gp_refine_stats* stats);
+
+/* GPU recount: exact directed cut and per-part loads (the semantics of
+ * tools/verify_partition.py:22-65 and src/graph.cpp:192-212). */
+gp_status gp_cut(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts,
+                 uint64_t* directed_cut, uint64_t* loads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
