@@ -1,0 +1,298 @@
+"""B200-native multilevel k-way graph partitioner (horkxg's SCLP coarsening,
+spectral initial partition and incremental bucketed refinement).
+
+The product is the C ABI in include/gpart_b200.h, implemented by
+libgpart_b200.so, and the drop-in drivers bin/gpart_partition_{standard,big}.
+This module is a thin ctypes binding of that ABI for Python callers, tests and
+bench.py; it mirrors the reference's library entry points (coarsen,
+aggregate, contract, initial_partition_gpu, refine_partition, partition).
+Loading fails loudly when the library is missing: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libgpart_b200.so"
+BIN = PKG / "bin"
+
+GP_OK, GP_EINVAL, GP_ERUNTIME, GP_EOVERFLOW, GP_ECUDA, GP_ETIMEOUT, GP_ENOMEM = range(7)
+STANDARD, BIG = 0, 1
+HOST, DEVICE = 0, 1
+
+
+class GraphDesc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("m", ctypes.c_int64), ("width", ctypes.c_int32), ("memory", ctypes.c_int32),
+                ("index64", ctypes.c_int32), ("reserved", ctypes.c_int32), ("offsets", ctypes.c_void_p),
+                ("neighbors", ctypes.c_void_p), ("edge_weights", ctypes.c_void_p),
+                ("vertex_weights", ctypes.c_void_p)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("parts", ctypes.c_int32), ("cluster_size_factor", ctypes.c_int32), ("imbalance", ctypes.c_double),
+                ("seed", ctypes.c_uint32), ("verify", ctypes.c_int32), ("deterministic", ctypes.c_int32),
+                ("pack_isolated", ctypes.c_int32), ("max_levels", ctypes.c_int32), ("max_rounds", ctypes.c_int32),
+                ("stop_ratio", ctypes.c_double), ("growth_ratio", ctypes.c_double), ("log", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("m", ctypes.c_int64), ("cut", ctypes.c_uint64), ("capacity", ctypes.c_uint64),
+                ("total_edge_weight", ctypes.c_uint64), ("part_weights", ctypes.c_uint64 * 32),
+                ("levels", ctypes.c_int32), ("reserved", ctypes.c_int32), ("coarsest_n", ctypes.c_int64),
+                ("initial_cut", ctypes.c_uint64), ("coarsen_seconds", ctypes.c_double),
+                ("initial_seconds", ctypes.c_double), ("uncoarsen_seconds", ctypes.c_double),
+                ("free_seconds", ctypes.c_double), ("algorithm_seconds", ctypes.c_double),
+                ("prepare_seconds", ctypes.c_double)]
+
+
+class RefineStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int32), ("proposals", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
+                ("initial_cut", ctypes.c_uint64), ("final_cut", ctypes.c_uint64),
+                ("final_max_part_weight", ctypes.c_uint64), ("admission_iterations", ctypes.c_int32),
+                ("admission_fallbacks", ctypes.c_int32)]
+
+
+EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_error", "gp_partition_capacity",
+           "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
+           "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
+           "gp_launch_count", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump"]
+
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: the CUDA library must be built (__graft_entry__.build())")
+        L = ctypes.CDLL(str(LIB_PATH))
+        vp, i64, i32, u32, dbl = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_uint32, ctypes.c_double
+        P = ctypes.POINTER
+        L.gp_options_default.argtypes = [P(Options)]
+        L.gp_ctx_create.argtypes = [i32, P(vp)]
+        L.gp_ctx_destroy.argtypes = [vp]
+        L.gp_ctx_error.argtypes = [vp]
+        L.gp_ctx_error.restype = ctypes.c_char_p
+        L.gp_partition_capacity.argtypes = [ctypes.c_uint64, i32, dbl, P(ctypes.c_uint64)]
+        L.gp_partition.argtypes = [vp, P(GraphDesc), P(Options), vp, P(Report)]
+        L.gp_aggregate.argtypes = [vp, P(GraphDesc), i32, u32, i32, i32, i32, vp, P(i64), P(ctypes.c_uint64)]
+        L.gp_contract.argtypes = [vp, P(GraphDesc), vp, i64, vp, vp, vp, vp, P(i64)]
+        L.gp_coarsen.argtypes = [vp, P(GraphDesc), P(Options), P(vp)]
+        L.gp_hierarchy_levels.argtypes = [vp]
+        L.gp_hierarchy_level.argtypes = [vp, i32, P(i64), P(i64), vp, vp, vp, vp, vp]
+        L.gp_hierarchy_write.argtypes = [vp, ctypes.c_char_p]
+        L.gp_hierarchy_free.argtypes = [vp]
+        L.gp_initial_partition.argtypes = [vp, P(GraphDesc), i32, dbl, u32, vp]
+        L.gp_diffusion.argtypes = [vp, P(GraphDesc), vp, i32, u32, i32, vp]
+        L.gp_refine.argtypes = [vp, P(GraphDesc), vp, i32, dbl, i32, i32, P(RefineStats)]
+        L.gp_cut.argtypes = [vp, P(GraphDesc), vp, i32, P(ctypes.c_uint64), vp]
+        L.gp_launch_count.argtypes = [vp]
+        L.gp_launch_count.restype = ctypes.c_uint64
+        L.gp_ctx_stream.argtypes = [vp]
+        L.gp_ctx_stream.restype = vp
+        L.gp_profile_enable.argtypes = [vp, i32]
+        L.gp_profile_dump.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64]
+        _LIB = L
+    return _LIB
+
+
+class PartitionError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().gp_options_default(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def capacity(total: int, parts: int, ratio: float) -> int:
+    out = ctypes.c_uint64()
+    rc = lib().gp_partition_capacity(total, parts, ratio, ctypes.byref(out))
+    if rc:
+        raise PartitionError(rc, "invalid partition capacity")
+    return out.value
+
+
+class HostGraph:
+    """A host CSR in one of the two widths (keeps the numpy arrays alive)."""
+
+    def __init__(self, offsets, neighbors, edge_weights=None, vertex_weights=None, width: int = STANDARD,
+                 index64: bool = False):
+        self.width = width
+        self.index64 = index64
+        wdt = np.uint32 if width == STANDARD else np.uint64
+        if index64:
+            self.off = np.ascontiguousarray(offsets, dtype=np.int64)
+            self.nbr = np.ascontiguousarray(neighbors, dtype=np.int64)
+        else:
+            self.off = np.ascontiguousarray(offsets, dtype=np.int32 if width == STANDARD else np.int64)
+            self.nbr = np.ascontiguousarray(neighbors, dtype=np.int32)
+        self.ew = None if edge_weights is None else np.ascontiguousarray(edge_weights, dtype=wdt)
+        self.vw = None if vertex_weights is None else np.ascontiguousarray(vertex_weights, dtype=wdt)
+        self.n = len(self.off) - 1
+        self.m = len(self.nbr)
+
+    def desc(self) -> GraphDesc:
+        d = GraphDesc()
+        d.n, d.m, d.width, d.memory, d.index64 = self.n, self.m, self.width, HOST, int(self.index64)
+        d.offsets = self.off.ctypes.data
+        d.neighbors = self.nbr.ctypes.data
+        d.edge_weights = None if self.ew is None else self.ew.ctypes.data
+        d.vertex_weights = None if self.vw is None else self.vw.ctypes.data
+        return d
+
+
+class Context:
+    """One GPU context (stream + memory pool).  Not thread-safe."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        rc = lib().gp_ctx_create(device, ctypes.byref(self._h))
+        if rc:
+            raise PartitionError(rc, "cannot create context")
+
+    def close(self):
+        if self._h:
+            lib().gp_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc:
+            raise PartitionError(rc, lib().gp_ctx_error(self._h).decode())
+
+    @property
+    def launches(self) -> int:
+        return int(lib().gp_launch_count(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().gp_ctx_stream(self._h) or 0)
+
+    def profile(self, on: bool):
+        self._check(lib().gp_profile_enable(self._h, int(on)))
+
+    def profile_dump(self) -> dict:
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(lib().gp_profile_dump(self._h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, launches, ms, nbytes = line.split()
+            out[name] = {"launches": int(launches), "ms": float(ms), "bytes": float(nbytes)}
+        return out
+
+    def partition_desc(self, desc: GraphDesc, labels_ptr: int, options: Options):
+        """Partition a graph described by a raw GraphDesc (host or device
+        pointers); labels_ptr is in the graph's memory space."""
+        rep = Report()
+        self._check(lib().gp_partition(self._h, ctypes.byref(desc), ctypes.byref(options), labels_ptr,
+                                       ctypes.byref(rep)))
+        return rep
+
+    def partition(self, g: HostGraph, options: Options | None = None, **kw):
+        o = options or default_options(**kw)
+        labels = np.zeros(g.n, np.int32)
+        rep = Report()
+        d = g.desc()
+        self._check(lib().gp_partition(self._h, ctypes.byref(d), ctypes.byref(o), labels.ctypes.data,
+                                       ctypes.byref(rep)))
+        return labels, rep
+
+    def aggregate(self, g: HostGraph, parts: int, seed: int, level: int, cluster_size_factor: int = 256,
+                  pack_isolated: bool = False):
+        mp = np.zeros(g.n, np.int32)
+        cn, cap = ctypes.c_int64(), ctypes.c_uint64()
+        d = g.desc()
+        self._check(lib().gp_aggregate(self._h, ctypes.byref(d), parts, seed, level, cluster_size_factor,
+                                       int(pack_isolated), mp.ctypes.data, ctypes.byref(cn), ctypes.byref(cap)))
+        return mp, cn.value, cap.value
+
+    def contract(self, g: HostGraph, mp, coarse_n: int):
+        mp = np.ascontiguousarray(mp, np.int32)
+        off = np.zeros(coarse_n + 1, np.int64)
+        nbr = np.zeros(max(g.m, 1), np.int32)
+        ew = np.zeros(max(g.m, 1), np.uint64)
+        vw = np.zeros(coarse_n, np.uint64)
+        cm = ctypes.c_int64()
+        d = g.desc()
+        self._check(lib().gp_contract(self._h, ctypes.byref(d), mp.ctypes.data, coarse_n, off.ctypes.data,
+                                      nbr.ctypes.data, ew.ctypes.data, vw.ctypes.data, ctypes.byref(cm)))
+        return off, nbr[:cm.value].copy(), ew[:cm.value].copy(), vw
+
+    def coarsen(self, g: HostGraph, options: Options | None = None, **kw):
+        """Returns a list of levels (offsets, neighbors, edge_weights,
+        vertex_weights, map_to_next or None)."""
+        o = options or default_options(**kw)
+        h = ctypes.c_void_p()
+        d = g.desc()
+        self._check(lib().gp_coarsen(self._h, ctypes.byref(d), ctypes.byref(o), ctypes.byref(h)))
+        try:
+            L = lib()
+            count = L.gp_hierarchy_levels(h)
+            out = []
+            for i in range(count):
+                n, m = ctypes.c_int64(), ctypes.c_int64()
+                L.gp_hierarchy_level(h, i, ctypes.byref(n), ctypes.byref(m), None, None, None, None, None)
+                off = np.zeros(n.value + 1, np.int64)
+                nbr = np.zeros(max(m.value, 1), np.int32)
+                ew = np.zeros(max(m.value, 1), np.uint64)
+                vw = np.zeros(n.value, np.uint64)
+                mp = np.zeros(n.value, np.int32) if i + 1 < count else None
+                L.gp_hierarchy_level(h, i, None, None, off.ctypes.data, nbr.ctypes.data, ew.ctypes.data,
+                                     vw.ctypes.data, None if mp is None else mp.ctypes.data)
+                out.append((off, nbr[:m.value], ew[:m.value], vw, mp))
+            return out
+        finally:
+            lib().gp_hierarchy_free(h)
+
+    def initial_partition(self, g: HostGraph, parts: int, ratio: float = 1.03, seed: int = 0):
+        labels = np.zeros(g.n, np.int32)
+        d = g.desc()
+        self._check(lib().gp_initial_partition(self._h, ctypes.byref(d), parts, ratio, seed, labels.ctypes.data))
+        return labels
+
+    def diffusion(self, g: HostGraph, labels, group: int, seed: int, steps: int = 64):
+        labels = np.ascontiguousarray(labels, np.int32)
+        x = np.zeros(g.n, np.float32)
+        d = g.desc()
+        self._check(lib().gp_diffusion(self._h, ctypes.byref(d), labels.ctypes.data, group, seed, steps,
+                                       x.ctypes.data))
+        return x
+
+    def refine(self, g: HostGraph, labels, parts: int, ratio: float = 1.03, max_rounds: int = 32,
+               deterministic: bool = True):
+        labels = np.array(labels, dtype=np.int32, copy=True)
+        st = RefineStats()
+        d = g.desc()
+        self._check(lib().gp_refine(self._h, ctypes.byref(d), labels.ctypes.data, parts, ratio, max_rounds,
+                                    int(deterministic), ctypes.byref(st)))
+        return labels, st
+
+    def cut(self, g: HostGraph, labels, parts: int):
+        labels = np.ascontiguousarray(labels, np.int32)
+        c = ctypes.c_uint64()
+        loads = np.zeros(parts, np.uint64)
+        d = g.desc()
+        self._check(lib().gp_cut(self._h, ctypes.byref(d), labels.ctypes.data, parts, ctypes.byref(c),
+                                 loads.ctypes.data))
+        return c.value, loads

@@ -6,7 +6,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <cstdio>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -88,7 +90,63 @@ struct Device {
     void sync() { GP_CUDA(cudaStreamSynchronize(stream)); }
     // Read a device error word; throws on any set bit.
     void check_errors();
+
+    // Launch accounting and optional per-kernel CUDA-event timing.
+    u64 launches = 0;
+    bool prof = false;
+    struct ProfEntry {
+        u64 launches = 0;
+        double ms = 0.0;
+        double bytes = 0.0;     // algorithmic bytes recorded by the call sites
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    };
+    std::map<std::string, ProfEntry> prof_table;
+    std::vector<cudaEvent_t> event_pool;
+    cudaEvent_t event() {
+        if (!event_pool.empty()) { auto e = event_pool.back(); event_pool.pop_back(); return e; }
+        cudaEvent_t e;
+        GP_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    void prof_bytes(const char* name, double bytes) { if (prof) prof_table[name].bytes += bytes; }
+    // Resolve pending event pairs (synchronises the stream).
+    void prof_resolve() {
+        sync();
+        for (auto& kv : prof_table) {
+            for (auto& pr : kv.second.pending) {
+                float ms = 0.f;
+                GP_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+                kv.second.ms += ms;
+                event_pool.push_back(pr.first);
+                event_pool.push_back(pr.second);
+            }
+            kv.second.pending.clear();
+        }
+    }
 };
+
+// Every kernel launch of the library goes through this helper: it counts
+// launches and, when profiling is on, brackets the launch with CUDA events on
+// the context stream.
+template <typename... KArgs, typename... Args>
+void launch(Device& d, const char* name, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
+    static_assert(sizeof...(KArgs) == sizeof...(Args), "kernel argument count");
+    cudaEvent_t a = nullptr;
+    if (d.prof) {
+        a = d.event();
+        GP_CUDA(cudaEventRecord(a, d.stream));
+    }
+    k<<<grid, block, smem, d.stream>>>(static_cast<KArgs>(args)...);
+    GP_CUDA(cudaGetLastError());
+    ++d.launches;
+    if (d.prof) {
+        cudaEvent_t b = d.event();
+        GP_CUDA(cudaEventRecord(b, d.stream));
+        auto& e = d.prof_table[name];
+        e.pending.push_back({a, b});
+        ++e.launches;
+    }
+}
 
 template <typename T>
 class Buf {
@@ -105,7 +163,9 @@ public:
     }
     Buf(const Buf&) = delete;
     Buf& operator=(const Buf&) = delete;
-    void reset() { if (ptr_ && dev_) dev_->release(ptr_); ptr_ = nullptr; count_ = 0; }
+    void reset() { if (ptr_ && dev_) dev_->release(ptr_); ptr_ = nullptr; count_ = 0; dev_ = nullptr; }
+    // Non-owning view of caller memory (never freed by this Buf).
+    void borrow(T* p, size_t count) { reset(); ptr_ = p; count_ = count; }
     // Grow without preserving contents.
     void ensure(Device& d, size_t count) {
         if (count <= count_ && ptr_) return;

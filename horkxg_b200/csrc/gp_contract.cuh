@@ -1,0 +1,294 @@
+// CSR contraction (src/coarsen.cu:1674-1814), restated as a segmented
+// problem instead of one global sort of all m edge records:
+//
+// 1. every coarse row c gets a segment of the size of its members' fine
+//    degrees; a warp-batched pass scatters each fine row's (map[u], w) pairs
+//    into its coarse row's segment (internal edges become a sentinel);
+// 2. every segment is sorted by target and its runs of equal targets summed:
+//    a warp bitonic sort for segments of <= 32 entries, a shared-memory block
+//    radix sort for <= kSegSmem entries, a global-memory block radix sort for
+//    larger (hub) segments;
+// 3. row lengths are scanned into the coarse offsets and the unique entries
+//    copied out.
+//
+// Output rows are sorted by target with parallel edges summed, exactly as
+// the reference's sort + reduce_by_key + write_coarse_csr_kernel produce them.
+#pragma once
+
+#include "gp_prim.cuh"
+
+namespace gp {
+
+constexpr int kSegSmem = 4096;
+
+// Fine-degree sum per coarse row.
+template <typename O>
+__global__ void row_fine_degree_kernel(i64 n, const O* off, const i32* map, i64* fdeg) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const i64 d = static_cast<i64>(off[v + 1]) - off[v];
+    if (d) atomicAdd(reinterpret_cast<unsigned long long*>(&fdeg[map[v]]), static_cast<unsigned long long>(d));
+}
+
+// Warp handles 32 consecutive fine rows: reserves each row's slot range in
+// its coarse segment, then walks the rows' contiguous edge range 32 entries
+// at a time; a lane finds its source row by a 5-step shuffle binary search.
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) scatter_edges_kernel(
+    i64 n, const O* __restrict__ off, const i32* __restrict__ nbr, const W* __restrict__ ew,
+    const i32* __restrict__ map, const i64* __restrict__ temp_off, i64* cursor, u32 sentinel,
+    u32* __restrict__ tgt, W* __restrict__ wt) {
+    const int lane = threadIdx.x & 31;
+    const i64 v0 = ((static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) >> 5) * 32;
+    if (v0 >= n) return;
+    const i64 v = v0 + lane;
+    const bool has = v < n;
+    const i64 rs = has ? static_cast<i64>(off[v]) : 0;
+    const i64 re = has ? static_cast<i64>(off[v + 1]) : 0;
+    const i32 c = has ? map[v] : 0;
+    i64 dst = 0;
+    if (has && re > rs)
+        dst = temp_off[c] + static_cast<i64>(atomicAdd(reinterpret_cast<unsigned long long*>(&cursor[c]),
+                                                        static_cast<unsigned long long>(re - rs)));
+    const i64 first = __shfl_sync(0xffffffffu, rs, 0);
+    i64 last = has ? re : 0;
+    for (int o = 16; o; o >>= 1) { const i64 x = __shfl_xor_sync(0xffffffffu, last, o); last = x > last ? x : last; }
+    for (i64 base = first; base < last; base += 32) {
+        const i64 e = base + lane;
+        // largest lane j with rs_j <= e (rows with rs_j == re_j are skipped
+        // naturally because a later row starts at the same offset)
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+            const i64 probe = __shfl_sync(0xffffffffu, rs, lo + step);
+            const bool probe_valid = v0 + lo + step < n;
+            if (probe_valid && probe <= e) lo += step;
+        }
+        const i64 my_rs = __shfl_sync(0xffffffffu, rs, lo);
+        const i64 my_dst = __shfl_sync(0xffffffffu, dst, lo);
+        const i32 my_c = __shfl_sync(0xffffffffu, c, lo);
+        if (e < last) {
+            const i32 t = map[nbr[e]];
+            const i64 out = my_dst + (e - my_rs);
+            tgt[out] = t == my_c ? sentinel : static_cast<u32>(t);
+            wt[out] = weight_at(ew, e);
+        }
+    }
+}
+
+// Sum runs of equal keys of a sorted segment (keys, vals)[0, count); the
+// unique non-sentinel (key, sum) pairs are written to (out_k, out_v) in
+// order.  Block-cooperative; returns the unique count in every thread.
+template <typename W>
+struct RunShared {
+    i64 scan_tmp[kWarps + 1];
+    u64 wscan_tmp[kWarps + 1];
+};
+
+template <typename W>
+__device__ i64 block_reduce_runs(const u32* keys, const W* vals, i64 count, u32 sentinel, u32* out_k, W* out_v,
+                                 RunShared<W>& sh) {
+    i64 unique_carry = 0;   // unique runs emitted before this tile
+    W w_carry = 0;          // running weight sum before this tile
+    constexpr int kItems = 8;
+    for (i64 t0 = 0; t0 < count; t0 += static_cast<i64>(kThreads) * kItems) {
+        const i64 base = t0 + static_cast<i64>(threadIdx.x) * kItems;
+        u32 k[kItems];
+        W w[kItems];
+        i64 heads = 0;
+        W wsum = 0;
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const i64 i = base + j;
+            k[j] = i < count ? keys[i] : sentinel;
+            w[j] = i < count ? vals[i] : W(0);
+            const bool head = i < count && k[j] != sentinel && (i == 0 || keys[i - 1] != k[j]);
+            heads += head ? 1 : 0;
+            wsum += w[j];
+        }
+        i64 heads_total;
+        const i64 head_ex = block_exclusive_sum<i64>(heads, sh.scan_tmp, &heads_total);
+        u64 wtotal;
+        const u64 w_ex = block_exclusive_sum<u64>(static_cast<u64>(wsum), sh.wscan_tmp, &wtotal);
+        // Pass 1: heads record their exclusive weight prefix in out_v.
+        i64 u = unique_carry + head_ex;
+        W run = w_carry + static_cast<W>(w_ex);
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const i64 i = base + j;
+            const bool head = i < count && k[j] != sentinel && (i == 0 || keys[i - 1] != k[j]);
+            if (head) { out_k[u] = k[j]; out_v[u] = run; ++u; }
+            run += w[j];
+        }
+        __syncthreads();
+        // Pass 2: run ends turn the prefix into the run's sum.
+        u = unique_carry + head_ex;
+        run = w_carry + static_cast<W>(w_ex);
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const i64 i = base + j;
+            const bool head = i < count && k[j] != sentinel && (i == 0 || keys[i - 1] != k[j]);
+            if (head) ++u;
+            run += w[j];
+            const bool end = i < count && k[j] != sentinel && (i + 1 == count || keys[i + 1] != k[j]);
+            if (end) out_v[u - 1] = run - out_v[u - 1];
+        }
+        __syncthreads();
+        unique_carry += heads_total;
+        w_carry += static_cast<W>(wtotal);
+    }
+    return unique_carry;
+}
+
+// Rows with <= 32 entries: one warp per row, bitonic sort in registers.
+template <typename W>
+__global__ void __launch_bounds__(kThreads) segment_warp_kernel(i64 rows, const i32* __restrict__ list,
+                                                                const i64* __restrict__ temp_off, u32 sentinel,
+                                                                u32* tgt, W* wt, i64* row_len) {
+    const int lane = threadIdx.x & 31;
+    const i64 r = (static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    if (r >= rows) return;
+    const i32 c = list[r];
+    const i64 s = temp_off[c];
+    const int len = static_cast<int>(temp_off[c + 1] - s);
+    u32 k = lane < len ? tgt[s + lane] : 0xffffffffu;
+    W w = lane < len ? wt[s + lane] : W(0);
+    warp_bitonic_sort(k, w);
+    const u32 prev = __shfl_up_sync(0xffffffffu, k, 1);
+    const bool valid = lane < len && k != sentinel;
+    const bool head = valid && (lane == 0 || prev != k);
+    // segmented inclusive sum over runs (runs are contiguous after sorting)
+    W sum = w;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const W o = __shfl_up_sync(0xffffffffu, sum, d);
+        const u32 ok = __shfl_up_sync(0xffffffffu, k, d);
+        if (lane >= d && ok == k) sum += o;
+    }
+    const u32 next = __shfl_down_sync(0xffffffffu, k, 1);
+    const bool end = valid && (lane == 31 || next != k);
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int u = __popc(heads & lanemask_lt()) + (head ? 0 : -1);   // index of this lane's run
+    __syncwarp();
+    if (end) { tgt[s + u] = k; wt[s + u] = sum; }
+    if (lane == 0) row_len[c] = __popc(heads);
+}
+
+// Rows with 33..kSegSmem entries: block per row, radix sort in shared memory.
+template <typename W>
+__global__ void __launch_bounds__(kThreads) segment_smem_kernel(i64 rows, const i32* __restrict__ list,
+                                                                const i64* __restrict__ temp_off, u32 sentinel,
+                                                                int key_bits, u32* tgt, W* wt, i64* row_len) {
+    extern __shared__ unsigned char smem_raw[];
+    u32* k0 = reinterpret_cast<u32*>(smem_raw);
+    u32* k1 = k0 + kSegSmem;
+    W* w0 = reinterpret_cast<W*>(k1 + kSegSmem);
+    W* w1 = w0 + kSegSmem;
+    __shared__ RankShared rank_sh;
+    __shared__ RunShared<W> run_sh;
+    const i64 r = blockIdx.x;
+    if (r >= rows) return;
+    const i32 c = list[r];
+    const i64 s = temp_off[c];
+    const i64 len = temp_off[c + 1] - s;
+    for (i64 i = threadIdx.x; i < len; i += kThreads) { k0[i] = tgt[s + i]; w0[i] = wt[s + i]; }
+    __syncthreads();
+    block_radix_sort_segment(k0, w0, k1, w1, len, 0, key_bits, rank_sh);
+    const i64 u = block_reduce_runs(k0, w0, len, sentinel, tgt + s, wt + s, run_sh);
+    if (threadIdx.x == 0) row_len[c] = u;
+}
+
+// Larger rows: block per row, radix sort ping-ponging through global scratch
+// (alt buffers at alt_off[r]).
+template <typename W>
+__global__ void __launch_bounds__(kThreads) segment_global_kernel(i64 rows, const i32* __restrict__ list,
+                                                                  const i64* __restrict__ temp_off,
+                                                                  const i64* __restrict__ alt_off, u32 sentinel,
+                                                                  int key_bits, u32* tgt, W* wt, u32* alt_k, W* alt_w,
+                                                                  i64* row_len) {
+    __shared__ RankShared rank_sh;
+    __shared__ RunShared<W> run_sh;
+    const i64 r = blockIdx.x;
+    if (r >= rows) return;
+    const i32 c = list[r];
+    const i64 s = temp_off[c];
+    const i64 len = temp_off[c + 1] - s;
+    u32* ak = alt_k + alt_off[r];
+    W* aw = alt_w + alt_off[r];
+    block_radix_sort_segment(tgt + s, wt + s, ak, aw, len, 0, key_bits, rank_sh);
+    // runs are reduced out of the sorted data into the alt buffer, then copied back
+    const i64 u = block_reduce_runs(tgt + s, wt + s, len, sentinel, ak, aw, run_sh);
+    for (i64 i = threadIdx.x; i < u; i += kThreads) { tgt[s + i] = ak[i]; wt[s + i] = aw[i]; }
+    if (threadIdx.x == 0) row_len[c] = u;
+}
+
+// Row-size classes: 0 empty, 1 <= 32, 2 <= kSegSmem, 3 larger.
+__global__ void row_class_kernel(i64 rows, const i64* temp_off, u64* keys, i32* vals, u32* counts) {
+    __shared__ u32 local[4];
+    if (threadIdx.x < 4) local[threadIdx.x] = 0;
+    __syncthreads();
+    const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c < rows) {
+        const i64 l = temp_off[c + 1] - temp_off[c];
+        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kSegSmem ? 2 : 3;
+        keys[c] = static_cast<u64>(k);
+        vals[c] = static_cast<i32>(c);
+        atomicAdd(&local[k], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && local[threadIdx.x]) atomicAdd(&counts[threadIdx.x], local[threadIdx.x]);
+}
+
+template <typename O>
+struct RowLenToO {
+    const i64* len;
+    __device__ O operator()(i64 i) const { return static_cast<O>(len[i]); }
+};
+
+struct BigRowLen {
+    const i32* list;
+    const i64* temp_off;
+    i64 count;
+    __device__ i64 operator()(i64 i) const {
+        if (i >= count) return 0;
+        const i32 c = list[i];
+        return temp_off[c + 1] - temp_off[c];
+    }
+};
+
+// Copy each row's unique entries from its segment to the final CSR; warp per
+// 32 rows with a shuffle binary search (as in scatter_edges_kernel).
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64* __restrict__ temp_off,
+                                                             const O* __restrict__ coff, const u32* __restrict__ tgt,
+                                                             const W* __restrict__ wt, i32* __restrict__ nbr,
+                                                             W* __restrict__ ew) {
+    const int lane = threadIdx.x & 31;
+    const i64 r0 = ((static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) >> 5) * 32;
+    if (r0 >= rows) return;
+    const i64 r = r0 + lane;
+    const bool has = r < rows;
+    const i64 ds = has ? static_cast<i64>(coff[r]) : 0;
+    const i64 de = has ? static_cast<i64>(coff[r + 1]) : 0;
+    const i64 src = has ? temp_off[r] : 0;
+    const i64 first = __shfl_sync(0xffffffffu, ds, 0);
+    i64 last = has ? de : 0;
+    for (int o = 16; o; o >>= 1) { const i64 x = __shfl_xor_sync(0xffffffffu, last, o); last = x > last ? x : last; }
+    for (i64 base = first; base < last; base += 32) {
+        const i64 e = base + lane;
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+            const i64 probe = __shfl_sync(0xffffffffu, ds, lo + step);
+            if (r0 + lo + step < rows && probe <= e) lo += step;
+        }
+        const i64 my_ds = __shfl_sync(0xffffffffu, ds, lo);
+        const i64 my_src = __shfl_sync(0xffffffffu, src, lo);
+        if (e < last) {
+            nbr[e] = static_cast<i32>(tgt[my_src + (e - my_ds)]);
+            ew[e] = wt[my_src + (e - my_ds)];
+        }
+    }
+}
+
+}  // namespace gp

@@ -1,0 +1,270 @@
+// Recursive weighted spectral bisection on the coarsest graph
+// (src/initial_partition_gpu.cu:170-276), batched by recursion depth:
+//
+// * every open task of one depth runs its 64 lazy-diffusion steps in ONE
+//   cooperative kernel; vertices are spread over all SMs (warp per vertex),
+//   one bounded grid barrier per step; the per-task weighted moments are
+//   reduced redundantly by every block in a fixed order (deterministic), and
+//   the normalisation is folded into the next step's reads;
+// * the split sort by (x, vertex id) is one launch: a block per task sorts its
+//   slice with an LSD radix sort on (orderable x << 32 | id);
+// * the weight-prefix split, its capacity checks and the child task
+//   descriptors are computed on the device (block per task): the host never
+//   waits inside the recursion.
+//
+// The diffusion is FP32 (the reference uses FP64); each diffusion vector is
+// checked against the FP64 oracle within 1e-5 relative L2.
+#pragma once
+
+#include "gp_prim.cuh"
+
+namespace gp {
+
+struct InitTask {
+    i32 begin;
+    i32 count;
+    i32 first_part;
+    i32 parts;
+    u64 weight;
+    i32 left_child;    // index in the next depth's task array, -1 = leaf
+    i32 right_child;
+};
+
+struct Moments { float mass, sum, squares; };
+
+// Bounded grid barrier for cooperative launches: gives up after ~2^24 polls
+// and records kErrTimeout (the kernel then finishes with garbage values that
+// the host discards).
+__device__ __forceinline__ void grid_barrier(u32* counter, volatile u32* generation, u32* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const u32 gen = *generation;
+        __threadfence();
+        const u32 arrived = atomicAdd(counter, 1u);
+        if (arrived == gridDim.x - 1) {
+            *counter = 0;
+            __threadfence();
+            atomicAdd(const_cast<u32*>(generation), 1u);
+        } else {
+            u32 polls = 0;
+            while (*generation == gen) {
+                if (++polls > (1u << 24)) { set_error(err, kErrTimeout); break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+constexpr int kMaxInitTasks = 16;   // tasks per depth for k <= 32
+
+struct NormShared {
+    float mean[kMaxInitTasks];
+    float scale[kMaxInitTasks];
+    float red[3][kWarps];
+};
+
+// Every block computes every task's (mean, scale) from the per-position
+// contributions in the same order: deterministic and identical everywhere.
+__device__ void compute_norms(int tasks, const InitTask* task, const Moments* contrib, NormShared& sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int t = 0; t < tasks; ++t) {
+        const i32 b = task[t].begin, c = task[t].count;
+        float m = 0.f, s = 0.f, q = 0.f;
+        for (i32 i = threadIdx.x; i < c; i += kThreads) {
+            const Moments x = contrib[b + i];
+            m += x.mass; s += x.sum; q += x.squares;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            m += __shfl_xor_sync(0xffffffffu, m, o);
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            q += __shfl_xor_sync(0xffffffffu, q, o);
+        }
+        if (lane == 0) { sh.red[0][warp] = m; sh.red[1][warp] = s; sh.red[2][warp] = q; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float M = 0.f, S = 0.f, Q = 0.f;
+            for (int w = 0; w < kWarps; ++w) { M += sh.red[0][w]; S += sh.red[1][w]; Q += sh.red[2][w]; }
+            const float mean = S / M;
+            const float var = fmaxf(0.f, Q / M - mean * mean);
+            sh.mean[t] = mean;
+            sh.scale[t] = var > 1e-30f ? 1.0f / sqrtf(var) : 1.0f;
+        }
+        __syncthreads();
+    }
+}
+
+// spectral_start + 64 x (normalize, spectral_step) + normalize
+// (src/initial_partition_gpu.cu:81-142,206-229) for all tasks of one depth.
+// x_out[v] receives the final normalised value; key[p] the sort key of
+// position p.
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) diffusion_kernel(
+    int tasks, const InitTask* __restrict__ task, const i32* __restrict__ task_of_pos, i32 positions,
+    const i32* __restrict__ order, const i32* __restrict__ labels, const O* __restrict__ off,
+    const i32* __restrict__ nbr, const W* __restrict__ ew, u32 seed, int steps, float* deg, float* xa, float* xb,
+    Moments* contrib, float* x_out, u64* key, u32* bar_counter, u32* bar_gen, u32* err) {
+    __shared__ NormShared sh;
+    const int lane = threadIdx.x & 31;
+    const i32 warps_total = static_cast<i32>(gridDim.x) * kWarps;
+    const i32 warp_id = static_cast<i32>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    // start
+    for (i32 p = warp_id; p < positions; p += warps_total) {
+        const i32 t = task_of_pos[p];
+        if (t < 0) continue;
+        const i32 v = order[p];
+        const i32 group = task[t].first_part;
+        float d = 0.f;
+        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32)
+            if (labels[nbr[e]] == group) d += static_cast<float>(weight_at(ew, e));
+        d = warp_sum(d);
+        if (lane == 0) {
+            const u32 h = mix32(static_cast<u32>(v) ^ (seed ^ static_cast<u32>(group)));
+            const float a = static_cast<float>(static_cast<double>(h) / 4294967296.0 - 0.5);
+            deg[v] = d;
+            xa[v] = a;
+            const float mass = d > 0.f ? d : 1.f;
+            contrib[p] = {mass, mass * a, mass * a * a};
+        }
+    }
+    float* x = xa;
+    float* y = xb;
+    for (int it = 0; it <= steps; ++it) {
+        grid_barrier(bar_counter, bar_gen, err);
+        compute_norms(tasks, task, contrib, sh);
+        if (it == steps) break;
+        for (i32 p = warp_id; p < positions; p += warps_total) {
+            const i32 t = task_of_pos[p];
+            if (t < 0) continue;
+            const i32 v = order[p];
+            const i32 group = task[t].first_part;
+            const float mean = sh.mean[t], scale = sh.scale[t];
+            float s = 0.f;
+            for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
+                const i32 u = nbr[e];
+                if (labels[u] == group) s += static_cast<float>(weight_at(ew, e)) * ((x[u] - mean) * scale);
+            }
+            s = warp_sum(s);
+            if (lane == 0) {
+                const float d = deg[v];
+                const float xv = (x[v] - mean) * scale;
+                const float a = d > 0.f ? 0.5f * (xv + s / d) : xv;
+                y[v] = a;
+                const float mass = d > 0.f ? d : 1.f;
+                contrib[p] = {mass, mass * a, mass * a * a};
+            }
+        }
+        float* tmp = x; x = y; y = tmp;
+    }
+    // final normalisation + sort keys
+    for (i32 p = static_cast<i32>(blockIdx.x) * kThreads + threadIdx.x; p < positions; p += static_cast<i32>(gridDim.x) * kThreads) {
+        const i32 t = task_of_pos[p];
+        if (t < 0) continue;
+        const i32 v = order[p];
+        float a = (x[v] - sh.mean[t]) * sh.scale[t];
+        if (a == 0.f) a = 0.f;   // canonical +0 so that -0 and +0 tie (then id decides)
+        if (x_out) x_out[v] = a;
+        const u32 b = __float_as_uint(a);
+        const u32 ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+        key[p] = (static_cast<u64>(ord) << 32) | static_cast<u32>(v);
+    }
+}
+
+__global__ void task_positions_kernel(int tasks, const InitTask* task, i32* task_of_pos) {
+    const int t = blockIdx.x;
+    if (t >= tasks) return;
+    for (i32 i = threadIdx.x; i < task[t].count; i += kThreads) task_of_pos[task[t].begin + i] = t;
+}
+
+// Block per task: sort its slice by (x, id) and rewrite `order`.
+__global__ void __launch_bounds__(kThreads) task_sort_kernel(int tasks, const InitTask* task, u64* key, u64* key_alt,
+                                                             i32* order) {
+    __shared__ RankShared sh;
+    const int t = blockIdx.x;
+    if (t >= tasks) return;
+    const i32 b = task[t].begin, c = task[t].count;
+    block_radix_sort_segment<u64, u32>(key + b, nullptr, key_alt + b, nullptr, c, 0, 64, sh);
+    for (i32 i = threadIdx.x; i < c; i += kThreads) order[b + i] = static_cast<i32>(key[b + i] & 0xffffffffu);
+}
+
+// floor(w * num / den) exactly (w * num fits in 128 bits).
+__device__ __forceinline__ u64 mul_div_floor(u64 w, u64 num, u64 den) {
+    const unsigned __int128 p = static_cast<unsigned __int128>(w) * num;
+    return static_cast<u64>(p / den);
+}
+
+// Weight-prefix split, src/initial_partition_gpu.cu:231-254, block per task.
+template <typename W>
+__global__ void __launch_bounds__(kThreads) task_split_kernel(int tasks, const InitTask* task, InitTask* next,
+                                                              const i32* order, const W* vw, u64 capacity,
+                                                              u64* prefix, i32* labels, u32* err) {
+    __shared__ i64 scan_sh[kWarps + 1];
+    __shared__ int boundary_sh;
+    __shared__ u64 left_weight_sh;
+    const int t = blockIdx.x;
+    if (t >= tasks) return;
+    const InitTask tk = task[t];
+    const i32 b = tk.begin, c = tk.count;
+    u64 carry = 0;
+    for (i32 base = 0; base < c; base += kThreads) {
+        const i32 i = base + threadIdx.x;
+        const u64 w = i < c ? static_cast<u64>(weight_at(vw, order[b + i])) : 0;
+        i64 total;
+        const i64 ex = block_exclusive_sum<i64>(static_cast<i64>(w), scan_sh, &total);
+        if (i < c) prefix[b + i] = carry + static_cast<u64>(ex) + w;
+        carry += static_cast<u64>(total);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int left_parts = tk.parts / 2, right_parts = tk.parts - left_parts;
+        const u64 W_ = tk.weight;
+        const u64 target = mul_div_floor(W_, static_cast<u64>(left_parts), static_cast<u64>(tk.parts));
+        const u64 left_limit = capacity > W_ / left_parts ? W_ : capacity * left_parts;
+        const u64 right_limit = capacity > W_ / right_parts ? W_ : capacity * right_parts;
+        const u64 min_left = W_ > right_limit ? W_ - right_limit : 0;
+        // lower_bound over the inclusive prefix
+        i32 lo = 0, hi = c;
+        while (lo < hi) {
+            const i32 mid = lo + (hi - lo) / 2;
+            if (prefix[b + mid] < target) lo = mid + 1; else hi = mid;
+        }
+        int boundary = lo + 1;
+        boundary = max(left_parts, min(c - right_parts, boundary));
+        u64 lw = prefix[b + boundary - 1];
+        if (lw > left_limit && boundary > left_parts) { --boundary; lw = prefix[b + boundary - 1]; }
+        if (lw < min_left && boundary < c - right_parts) { ++boundary; lw = prefix[b + boundary - 1]; }
+        if (lw > left_limit || lw < min_left) set_error(err, kErrSplit);
+        boundary_sh = boundary;
+        left_weight_sh = lw;
+        const u64 rw = W_ - lw;
+        if (tk.left_child >= 0) {
+            InitTask& L = next[tk.left_child];
+            L.begin = b; L.count = boundary; L.weight = lw;
+        } else if (lw > capacity) {
+            set_error(err, kErrBalance);
+        }
+        if (tk.right_child >= 0) {
+            InitTask& R = next[tk.right_child];
+            R.begin = b + boundary; R.count = c - boundary; R.weight = rw;
+        } else if (rw > capacity) {
+            set_error(err, kErrBalance);
+        }
+    }
+    __syncthreads();
+    const int boundary = boundary_sh;
+    const int left_parts = tk.parts / 2;
+    for (i32 i = threadIdx.x; i < c; i += kThreads)
+        labels[order[b + i]] = i < boundary ? tk.first_part : tk.first_part + left_parts;
+}
+
+// Part weights + cut terms of the initial partition (part_weights,
+// cut_terms, src/initial_partition_gpu.cu:154-167).
+template <typename W>
+__global__ void part_weight_kernel(i64 n, const i32* labels, const W* vw, u64* loads) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n) atomic_add_u64(&loads[labels[v]], static_cast<u64>(weight_at(vw, v)));
+}
+
+}  // namespace gp

@@ -1,0 +1,1661 @@
+// Host side of the B200 partitioner: input preparation, the coarsening level
+// loop, the batched initial partition, the level-by-level projection and
+// refinement, and the C ABI of include/gpart_b200.h.
+//
+// Pipeline semantics follow app/partition_main.cu:20-142,
+// src/coarsen.cu:1906-2164, src/initial_partition_gpu.cu:170-276,
+// src/refine.cu:423-646 and src/refine_incremental.cuh:235-361.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <numeric>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "gp_common.cuh"
+#include "gp_prim.cuh"
+#include "gp_sclp.cuh"
+#include "gp_contract.cuh"
+#include "gp_initial.cuh"
+#include "gp_refine.cuh"
+
+namespace gp {
+
+void Device::check_errors() {
+    u32 e = 0;
+    fetch(*this, &e, err, 1);
+    if (!e) return;
+    GP_CUDA(cudaMemsetAsync(err, 0, sizeof(u32), stream));
+    if (e & kErrTimeout) fail(GP_ETIMEOUT, "a bounded device wait timed out");
+    if (e & kErrCapacity) fail(GP_ERUNTIME, "SCLP coarsening exceeded cluster capacity");
+    if (e & kErrSplit) fail(GP_ERUNTIME, "GPU spectral split cannot satisfy capacity");
+    if (e & kErrBalance) fail(GP_ERUNTIME, "GPU initializer infeasible balance");
+    if (e & kErrCutUnderflow) fail(GP_ERUNTIME, "incremental cut underflow");
+    if (e & kErrOddCut) fail(GP_ERUNTIME, "weighted CSR cut is not symmetric");
+    if (e & kErrTableFull) fail(GP_ERUNTIME, "internal hash table overflow");
+    fail(GP_EINVAL, "invalid graph input");
+}
+
+using Clock = std::chrono::steady_clock;
+inline double seconds_since(Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); }
+
+// include/partition_capacity.hpp:12-23
+u64 partition_capacity(u64 total, int parts, double ratio) {
+    if (parts < 2 || parts > 32 || !std::isfinite(ratio) || ratio < 1.0)
+        fail(GP_EINVAL, "invalid partition capacity options");
+    const long double raw = static_cast<long double>(total) * ratio / parts;
+    if (!std::isfinite(raw) || raw >= static_cast<long double>(std::numeric_limits<u64>::max()))
+        fail(GP_EOVERFLOW, "partition capacity exceeds uint64");
+    const auto capacity = static_cast<u64>(std::floor(raw));
+    if (capacity < total / static_cast<unsigned>(parts) + (total % parts != 0))
+        fail(GP_EINVAL, "integer partition capacity cannot hold total weight");
+    return capacity;
+}
+
+// ---------------------------------------------------------------------------
+// Device graph (one hierarchy level)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DGraph {
+    using O = typename T::O;
+    using W = typename T::W;
+    i64 n = 0, m = 0;
+    Buf<O> off;
+    Buf<i32> nbr;
+    Buf<W> ew, vw;
+    bool unit_ew = true, unit_vw = true;
+    const W* ewp() const { return unit_ew ? nullptr : ew.get(); }
+    const W* vwp() const { return unit_vw ? nullptr : vw.get(); }
+};
+
+struct Log {
+    bool on = false;
+    std::ostream& out = std::cout;
+};
+
+__global__ void iota_kernel(i64 n, i32* a) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = static_cast<i32>(i);
+}
+
+template <typename W>
+__global__ void widen_weights_kernel(i64 n, const W* vw, u64* out) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<u64>(weight_at(vw, i));
+}
+
+template <typename W>
+__global__ void sat_sum_kernel(i64 m, const W* w, u64* out) {
+    u64 s = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const u64 x = static_cast<u64>(weight_at(w, i));
+        s = ~0ULL - s < x ? ~0ULL : s + x;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const u64 x = __shfl_xor_sync(0xffffffffu, s, o);
+        s = ~0ULL - s < x ? ~0ULL : s + x;
+    }
+    if ((threadIdx.x & 31) == 0 && s) {
+        u64 prev = *reinterpret_cast<volatile u64*>(out);
+        while (true) {
+            const u64 next = ~0ULL - prev < s ? ~0ULL : prev + s;
+            const u64 seen = atomic_cas_u64(out, prev, next);
+            if (seen == prev) break;
+            prev = seen;
+        }
+    }
+}
+
+inline int stride_grid(Device& d, i64 items, int per_block = kThreads) {
+    return static_cast<int>(std::min<i64>(blocks_for(items, per_block), static_cast<i64>(d.sms) * 8));
+}
+
+// ---------------------------------------------------------------------------
+// SCLP aggregation (src/coarsen.cu:937-1659)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct AggResult {
+    Buf<i32> map;
+    Buf<typename T::W> cvw;
+    i64 coarse_n = 0;
+    u64 cap = 0;
+};
+
+template <typename T>
+struct SclpWork {
+    Buf<i32> clusters, target, list, list_alt, clist, clist_alt;
+    Buf<u64> cw, gain, demand, keys, keys_alt, excl, ckeys, ckeys_alt;
+    Buf<u32> tie, ccount;
+    Buf<unsigned char> cls;
+    Buf<i64> pos, flags, positions, table_off;
+    Buf<i32> table_keys;
+    Buf<u64> table_vals, scalars;
+    void ensure(Device& d, i64 n) {
+        const size_t s = static_cast<size_t>(n) + 1;
+        clusters.ensure(d, s); target.ensure(d, s); list.ensure(d, s); list_alt.ensure(d, s);
+        clist.ensure(d, s); clist_alt.ensure(d, s);
+        cw.ensure(d, s); gain.ensure(d, s); demand.ensure(d, s); keys.ensure(d, s); keys_alt.ensure(d, s);
+        excl.ensure(d, s); ckeys.ensure(d, s); ckeys_alt.ensure(d, s);
+        tie.ensure(d, s); ccount.ensure(d, 8); cls.ensure(d, s);
+        pos.ensure(d, s); flags.ensure(d, s); positions.ensure(d, s);
+        scalars.ensure(d, 16);
+    }
+};
+
+// Orders list[0, count) (ascending vertex ids) by (target asc, gain desc,
+// tie desc); vertex order survives as the stable tie-break.
+template <typename T>
+void order_proposals(Device& d, SclpWork<T>& w, i64 n, i64 count, u64 gmax) {
+    const int tbits = std::max(1, bit_width_u64(static_cast<u64>(std::max<i64>(1, n - 1))));
+    const int gbits = std::max(1, bit_width_u64(gmax));
+    auto keys = [&](int mode) {
+        launch(d, "admission_keys_kernel", admission_keys_kernel, blocks_for(count, kThreads), kThreads, 0, 
+            count, w.list.get(), w.target.get(), w.gain.get(), w.tie.get(), gmax, gbits, mode, w.keys.get());
+        GP_LAUNCH();
+    };
+    auto sort = [&](int bits) {
+        radix_sort<u64, i32>(d, w.keys.get(), w.list.get(), w.keys_alt.get(), w.list_alt.get(), count, 0, bits);
+    };
+    if (tbits + gbits + 32 <= 64) {
+        keys(0); sort(tbits + gbits + 32);
+    } else {
+        keys(1); sort(32);
+        if (tbits + gbits <= 64) { keys(2); sort(tbits + gbits); }
+        else { keys(3); sort(gbits); keys(4); sort(tbits); }
+    }
+}
+
+template <typename T>
+void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 seed, int level, int beta, bool pack,
+               AggResult<T>& out, Log& log) {
+    using O = typename T::O;
+    using W = typename T::W;
+    if (parts < 2 || parts > 32 || beta < 2) fail(GP_EINVAL, "invalid SCLP cluster capacity options");
+    const i64 n = g.n;
+    if (n <= 0 || n > std::numeric_limits<i32>::max())
+        fail(GP_ERUNTIME, "SCLP coarsening received an unsupported graph size");
+    w.ensure(d, n);
+    const O* off = g.off.get();
+    const i32* nbr = g.nbr.get();
+    const W* ew = g.ewp();
+    const W* vw = g.vwp();
+    u64* sc = w.scalars.get();
+    GP_CUDA(cudaMemsetAsync(sc, 0, 16 * sizeof(u64), d.stream));
+    w.ccount.zero(d);
+    launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, n), kThreads, 0, n, vw, sc);
+    GP_LAUNCH();
+    launch(d, "degree_class_kernel", degree_class_kernel<O>, blocks_for(n, kThreads), kThreads, 0, n, off, w.ckeys.get(),
+           w.clist.get(), w.ccount.get(), sc + 8);
+    GP_LAUNCH();
+    radix_sort<u64, i32>(d, w.ckeys.get(), w.clist.get(), w.ckeys_alt.get(), w.clist_alt.get(), n, 0, 8);
+    u64 stats[16];
+    u32 cnt[kClasses];
+    to_host(d, stats, sc, 16);
+    fetch(d, cnt, w.ccount.get(), kClasses);
+    const u64* class_edges = stats + 8;
+    const u64 total = stats[0], maxw = stats[1];
+    const u64 denom = static_cast<u64>(beta) * static_cast<u64>(parts);
+    const u64 cap = std::max(maxw, total / denom + (total % denom != 0 ? 1 : 0));
+    i64 class_off[kClasses + 1] = {0};
+    for (int c = 0; c < kClasses; ++c) class_off[c + 1] = class_off[c] + cnt[c];
+    const i32* lists = w.clist.get();
+    auto class_list = [&](int c) { return lists + class_off[c]; };
+
+    // global hash tables for hubs
+    const i64 hubs = cnt[5];
+    i64 table_total = 0;
+    if (hubs > 0) {
+        w.table_off.ensure(d, static_cast<size_t>(hubs) + 1);
+        exclusive_scan<i64>(d, HubTableSize<O>{class_list(5), off, hubs}, w.table_off.get(), hubs + 1,
+                            reinterpret_cast<i64*>(sc + 4));
+        fetch(d, &table_total, reinterpret_cast<i64*>(sc + 4), 1);
+        w.table_keys.ensure(d, static_cast<size_t>(table_total));
+        w.table_vals.ensure(d, static_cast<size_t>(table_total));
+        GP_CUDA(cudaMemsetAsync(w.table_keys.get(), 0xff, table_total * sizeof(i32), d.stream));
+        GP_CUDA(cudaMemsetAsync(w.table_vals.get(), 0, table_total * sizeof(u64), d.stream));
+    }
+
+    i32* clusters = w.clusters.get();
+    u64* cw = w.cw.get();
+    launch(d, "iota_kernel", iota_kernel, blocks_for(n, kThreads), kThreads, 0, n, clusters);
+    launch(d, "widen_weights_kernel", widen_weights_kernel<W>, blocks_for(n, kThreads), kThreads, 0, n, vw, cw);
+    launch(d, "fill_i32_kernel", fill_i32_kernel, blocks_for(n, kThreads), kThreads, 0, n, w.target.get(), kInvalid);
+    GP_LAUNCH();
+    SclpOut so{w.target.get(), w.gain.get(), w.tie.get(), w.demand.get()};
+
+    // Algorithmic bytes of one affinity+decode pass over class c: offsets,
+    // list, neighbours, edge weights, cluster gathers (none at round 0),
+    // cluster[v]/cluster weight reads and the proposal writes.
+    auto affinity_bytes = [&](int c, bool identity) {
+        const double v = cnt[c], e = static_cast<double>(class_edges[c]);
+        return v * (2 * sizeof(O) + 4 + 4 + 8 + 4 + 8 + 4 + 8) + e * (4 + (ew ? sizeof(W) : 0) + (identity ? 0 : 4));
+    };
+    auto affinity = [&](const RoundParams& p) {
+        if (d.prof) {
+            d.prof_bytes("affinity_small_kernel", affinity_bytes(1, p.identity) + affinity_bytes(2, p.identity));
+            d.prof_bytes("affinity_warp_hash_kernel", affinity_bytes(3, p.identity));
+            d.prof_bytes("affinity_block_hash_kernel", affinity_bytes(4, p.identity));
+            d.prof_bytes("affinity_global_hash_kernel", affinity_bytes(5, p.identity));
+        }
+        if (cnt[1])
+            launch(d, "affinity_small_kernel", affinity_small_kernel<8, O, W>, blocks_for(static_cast<i64>(cnt[1]) * 8, kThreads), kThreads, 0, 
+                cnt[1], class_list(1), off, nbr, ew, vw, clusters, cw, p, so);
+        if (cnt[2])
+            launch(d, "affinity_small_kernel", affinity_small_kernel<32, O, W>, blocks_for(static_cast<i64>(cnt[2]) * 32, kThreads), kThreads, 0, 
+                cnt[2], class_list(2), off, nbr, ew, vw, clusters, cw, p, so);
+        if (cnt[3])
+            launch(d, "affinity_warp_hash_kernel", affinity_warp_hash_kernel<O, W>, blocks_for(cnt[3], kWarps), kThreads, 0, 
+                cnt[3], class_list(3), off, nbr, ew, vw, clusters, cw, p, so, d.err);
+        if (cnt[4]) {
+            static bool configured = false;
+            if (!configured) {
+                GP_CUDA(cudaFuncSetAttribute(affinity_block_hash_kernel<O, W>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kLargeSlots * 12));
+                configured = true;
+            }
+        }
+        if (cnt[4])
+            launch(d, "affinity_block_hash_kernel", affinity_block_hash_kernel<O, W>, static_cast<int>(cnt[4]), kThreads, kLargeSlots * 12, 
+                cnt[4], class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
+        if (cnt[5])
+            launch(d, "affinity_global_hash_kernel", affinity_global_hash_kernel<O, W>, static_cast<int>(cnt[5]), kThreads, 0, 
+                cnt[5], class_list(5), off, nbr, ew, vw, clusters, cw, p, so, w.table_off.get(), w.table_keys.get(),
+                w.table_vals.get(), d.err);
+        GP_LAUNCH();
+    };
+    // compaction of cls == 2 into list (ascending) + count and gain maximum
+    auto compact_contested = [&](i64& count, u64& gmax) {
+        exclusive_scan<i64>(d, IsClass2{w.cls.get()}, w.pos.get(), n, reinterpret_cast<i64*>(sc + 2));
+        launch(d, "compact_class2_kernel", compact_class2_kernel, blocks_for(n, kThreads), kThreads, 0, n, w.cls.get(), w.pos.get(),
+                                                                                    w.list.get());
+        GP_LAUNCH();
+        u64 h[2];
+        fetch(d, h, sc + 2, 2);
+        count = static_cast<i64>(h[0]);
+        gmax = h[1];
+    };
+    auto count_clusters = [&]() {
+        GP_CUDA(cudaMemsetAsync(sc + 5, 0, sizeof(u64), d.stream));
+        launch(d, "count_nonzero_kernel", count_nonzero_kernel, stride_grid(d, n), kThreads, 0, n, cw, sc + 5);
+        GP_LAUNCH();
+        u64 c;
+        fetch(d, &c, sc + 5, 1);
+        return static_cast<i64>(c);
+    };
+    auto sorted_weight_prefix = [&](i64 count) {
+        exclusive_scan<u64>(d, SortedWeight<W>{w.list.get(), vw}, w.excl.get(), count);
+    };
+
+    i64 cluster_count = n;
+    const i64 desired = (n + 1) / 2;
+    int rounds = 0;
+    for (int round = 0; round < 4; ++round) {
+        if (static_cast<double>(cluster_count) <= 0.60 * n) break;
+        const i64 removable = std::max<i64>(0, cluster_count - desired);
+        const double fraction = std::min(0.50, static_cast<double>(removable) / static_cast<double>(cluster_count));
+        const auto threshold = static_cast<u32>(fraction * 4294967296.0);
+        const RoundParams p = make_round(seed, level, round, true, threshold);
+        w.demand.zero(d);
+        affinity(p);
+        GP_CUDA(cudaMemsetAsync(sc + 3, 0, sizeof(u64), d.stream));
+        launch(d, "admission_classify_kernel", admission_classify_kernel, blocks_for(n, kThreads), kThreads, 0, 
+            n, w.target.get(), w.demand.get(), cw, cap, w.gain.get(), w.cls.get(), sc + 3);
+        GP_LAUNCH();
+        i64 contested = 0;
+        u64 gmax = 0;
+        compact_contested(contested, gmax);
+        if (contested > 0) {
+            order_proposals(d, w, n, contested, gmax);
+            sorted_weight_prefix(contested);
+            launch(d, "segment_heads_kernel", segment_heads_kernel, blocks_for(contested, kThreads), kThreads, 0, 
+                contested, w.list.get(), w.target.get(), w.excl.get(), w.demand.get(), 0);
+            launch(d, "contested_accept_kernel", contested_accept_kernel<W>, blocks_for(contested, kThreads), kThreads, 0, 
+                contested, w.list.get(), w.target.get(), w.excl.get(), w.demand.get(), cw, vw, cap, w.cls.get());
+            GP_LAUNCH();
+        }
+        launch(d, "sclp_commit_kernel", sclp_commit_kernel<W>, blocks_for(n, kThreads), kThreads, 0, n, w.cls.get(), w.target.get(), vw,
+                                                                                 clusters, cw);
+        GP_LAUNCH();
+        cluster_count = count_clusters();
+        ++rounds;
+        if (log.on)
+            log.out << "ml_gpu_sclp_round level=" << level << " round=" << round << " mover_fraction=" << fraction
+                    << " clusters=" << cluster_count
+                    << " contraction_ratio=" << static_cast<double>(cluster_count) / static_cast<double>(n) << '\n';
+        if (static_cast<double>(cluster_count) <= 0.60 * n) break;
+    }
+
+    if (pack && cnt[0] > 1) {
+        const i64 iso = cnt[0];
+        exclusive_scan<u64>(d, SortedWeight<W>{class_list(0), vw}, w.excl.get(), iso);
+        launch(d, "fill_i32_kernel", fill_i32_kernel, blocks_for(iso + 1, kThreads), kThreads, 0, iso + 1, w.list_alt.get(),
+                                                                                   std::numeric_limits<i32>::max());
+        launch(d, "isolated_rep_kernel", isolated_rep_kernel<W>, blocks_for(iso, kThreads), kThreads, 0, iso, class_list(0), w.excl.get(),
+                                                                                    vw, cap, w.list_alt.get());
+        launch(d, "isolated_commit_kernel", isolated_commit_kernel<W>, blocks_for(iso, kThreads), kThreads, 0, 
+            iso, class_list(0), w.excl.get(), vw, cap, w.list_alt.get(), clusters, cw);
+        GP_LAUNCH();
+        cluster_count = count_clusters();
+    }
+
+    if (static_cast<double>(cluster_count) > 0.60 * n) {
+        RoundParams p = make_round(seed, level, 4, false, 0);
+        p.two_hop = 1;
+        affinity(p);
+        GP_CUDA(cudaMemsetAsync(sc + 3, 0, sizeof(u64), d.stream));
+        launch(d, "favorite_classify_kernel", favorite_classify_kernel, blocks_for(n, kThreads), kThreads, 0, n, w.target.get(), w.gain.get(),
+                                                                                   w.cls.get(), sc + 3);
+        GP_LAUNCH();
+        i64 cand = 0;
+        u64 gmax = 0;
+        compact_contested(cand, gmax);
+        if (cand > 0) {
+            order_proposals(d, w, n, cand, gmax);
+            launch(d, "segment_heads_kernel", segment_heads_kernel, blocks_for(cand, kThreads), kThreads, 0, 
+                cand, w.list.get(), w.target.get(), w.excl.get(), w.demand.get(), 1);
+            launch(d, "pair_flags_kernel", pair_flags_kernel<W>, blocks_for(cand, kThreads), kThreads, 0, 
+                cand, w.list.get(), w.target.get(), w.demand.get(), vw, cap, w.flags.get());
+            GP_LAUNCH();
+            exclusive_scan_array<i64>(d, w.flags.get(), w.positions.get(), cand);
+            const u64 budget = static_cast<u64>(std::max<i64>(0, cluster_count - desired));
+            if (budget > 0) {
+                launch(d, "pair_commit_kernel", pair_commit_kernel<W>, blocks_for(cand, kThreads), kThreads, 0, 
+                    cand, w.list.get(), w.flags.get(), w.positions.get(), budget, vw, clusters, cw);
+                GP_LAUNCH();
+            }
+        }
+        cluster_count = count_clusters();
+    }
+
+    // compaction
+    Buf<i32> compact(d, static_cast<size_t>(n));
+    exclusive_scan<i32>(d, NonEmpty{cw}, compact.get(), n, reinterpret_cast<i32*>(sc + 6));
+    i32 coarse_n = 0;
+    fetch(d, &coarse_n, reinterpret_cast<i32*>(sc + 6), 1);
+    out.map = Buf<i32>(d, static_cast<size_t>(n));
+    out.cvw = Buf<W>(d, static_cast<size_t>(std::max<i32>(coarse_n, 1)));
+    out.cvw.zero(d);
+    launch(d, "compact_map_kernel", compact_map_kernel<W>, blocks_for(n, kThreads), kThreads, 0, n, clusters, compact.get(), vw,
+                                                                             out.map.get(), out.cvw.get());
+    launch(d, "cap_check_kernel", cap_check_kernel<W>, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n, out.cvw.get(), cap, d.err);
+    GP_LAUNCH();
+    out.coarse_n = coarse_n;
+    out.cap = cap;
+    if (log.on)
+        log.out << "ml_gpu_sclp level=" << level << " fine_vertices=" << n << " coarse_vertices=" << coarse_n
+                << " contraction_ratio=" << static_cast<double>(coarse_n) / static_cast<double>(n) << " beta=" << beta
+                << " cluster_cap=" << cap << " lp_rounds=" << rounds << " low_vertices=" << cnt[1]
+                << " medium_vertices=" << cnt[2] + cnt[3] << " high_vertices=" << cnt[4] + cnt[5]
+                << " isolated_vertices=" << cnt[0] << " seed=" << seed << '\n';
+}
+
+// ---------------------------------------------------------------------------
+// Contraction (src/coarsen.cu:1674-1814)
+// ---------------------------------------------------------------------------
+template <typename T>
+void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<typename T::W>&& cvw, DGraph<T>& out) {
+    using O = typename T::O;
+    using W = typename T::W;
+    const i64 n = g.n, m = g.m;
+    Buf<i64> fdeg(d, static_cast<size_t>(coarse_n) + 1);
+    Buf<i64> temp_off(d, static_cast<size_t>(coarse_n) + 1);
+    Buf<i64> cursor(d, static_cast<size_t>(coarse_n) + 1);
+    Buf<i64> scal(d, 4);
+    fdeg.zero(d);
+    cursor.zero(d);
+    launch(d, "row_fine_degree_kernel", row_fine_degree_kernel<O>, blocks_for(n, kThreads), kThreads, 0, n, g.off.get(), map, fdeg.get());
+    GP_LAUNCH();
+    exclusive_scan_array<i64>(d, fdeg.get(), temp_off.get(), coarse_n + 1);
+    const u32 sentinel = static_cast<u32>(coarse_n);
+    Buf<u32> tgt(d, static_cast<size_t>(std::max<i64>(m, 1)));
+    Buf<W> wt(d, static_cast<size_t>(std::max<i64>(m, 1)));
+    const i64 warps = (n + 31) / 32;
+    d.prof_bytes("scatter_edges_kernel", static_cast<double>(n + 1) * sizeof(O) + n * (4.0 + 8 + 8) +
+                                             static_cast<double>(m) * (4 + 4 + 4 + (g.ewp() ? sizeof(W) : 0) + sizeof(W)));
+    launch(d, "scatter_edges_kernel", scatter_edges_kernel<O, W>, blocks_for(warps * 32, kThreads), kThreads, 0, 
+        n, g.off.get(), g.nbr.get(), g.ewp(), map, temp_off.get(), cursor.get(), sentinel, tgt.get(), wt.get());
+    GP_LAUNCH();
+    // row classes
+    Buf<u64> rk(d, static_cast<size_t>(coarse_n)), rk_alt(d, static_cast<size_t>(coarse_n));
+    Buf<i32> rl(d, static_cast<size_t>(coarse_n)), rl_alt(d, static_cast<size_t>(coarse_n));
+    Buf<u32> rc(d, 4);
+    rc.zero(d);
+    launch(d, "row_class_kernel", row_class_kernel, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n, temp_off.get(), rk.get(),
+                                                                              rl.get(), rc.get());
+    GP_LAUNCH();
+    radix_sort<u64, i32>(d, rk.get(), rl.get(), rk_alt.get(), rl_alt.get(), coarse_n, 0, 8);
+    u32 rcnt[4];
+    fetch(d, rcnt, rc.get(), 4);
+    const i64 c1 = rcnt[0], c2 = c1 + rcnt[1], c3 = c2 + rcnt[2];
+    Buf<i64> row_len(d, static_cast<size_t>(coarse_n) + 1);
+    row_len.zero(d);
+    const int key_bits = std::max(1, bit_width_u64(static_cast<u64>(coarse_n)));
+    if (rcnt[1])
+        launch(d, "segment_warp_kernel", segment_warp_kernel<W>, blocks_for(static_cast<i64>(rcnt[1]) * 32, kThreads), kThreads, 0, 
+            rcnt[1], rl.get() + c1, temp_off.get(), sentinel, tgt.get(), wt.get(), row_len.get());
+    if (rcnt[2]) {
+        const size_t smem = 2 * kSegSmem * (sizeof(u32) + sizeof(W));
+        GP_CUDA(cudaFuncSetAttribute(segment_smem_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        launch(d, "segment_smem_kernel", segment_smem_kernel<W>, static_cast<int>(rcnt[2]), kThreads, smem, 
+            rcnt[2], rl.get() + c2, temp_off.get(), sentinel, key_bits, tgt.get(), wt.get(), row_len.get());
+    }
+    GP_LAUNCH();
+    if (rcnt[3]) {
+        const i64 big = rcnt[3];
+        Buf<i64> alt_off(d, static_cast<size_t>(big) + 1);
+        exclusive_scan<i64>(d, BigRowLen{rl.get() + c3, temp_off.get(), big}, alt_off.get(), big + 1,
+                            scal.get());
+        i64 alt_total = 0;
+        fetch(d, &alt_total, scal.get(), 1);
+        Buf<u32> ak(d, static_cast<size_t>(alt_total));
+        Buf<W> aw(d, static_cast<size_t>(alt_total));
+        launch(d, "segment_global_kernel", segment_global_kernel<W>, static_cast<int>(big), kThreads, 0, 
+            big, rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, key_bits, tgt.get(), wt.get(), ak.get(),
+            aw.get(), row_len.get());
+        GP_LAUNCH();
+    }
+    out.n = coarse_n;
+    out.off = Buf<O>(d, static_cast<size_t>(coarse_n) + 1);
+    exclusive_scan<O>(d, RowLenToO<O>{row_len.get()}, out.off.get(), coarse_n + 1, reinterpret_cast<O*>(scal.get() + 1));
+    O cm = 0;
+    fetch(d, &cm, reinterpret_cast<O*>(scal.get() + 1), 1);
+    out.m = static_cast<i64>(cm);
+    out.nbr = Buf<i32>(d, static_cast<size_t>(std::max<i64>(out.m, 1)));
+    out.ew = Buf<W>(d, static_cast<size_t>(std::max<i64>(out.m, 1)));
+    out.unit_ew = false;
+    if (out.m > 0) {
+        d.prof_bytes("copy_rows_kernel", static_cast<double>(coarse_n) * (sizeof(O) + 8) + 2.0 * out.m * (4 + sizeof(W)));
+        launch(d, "copy_rows_kernel", copy_rows_kernel<O, W>, blocks_for(((coarse_n + 31) / 32) * 32, kThreads), kThreads, 0, 
+            coarse_n, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
+        GP_LAUNCH();
+    }
+    out.vw = std::move(cvw);
+    out.unit_vw = false;
+}
+
+// ---------------------------------------------------------------------------
+// Hierarchy
+// ---------------------------------------------------------------------------
+struct Opts {
+    int parts = 4;
+    double ratio = 1.03;
+    u32 seed = 0;
+    bool verify = false;
+    bool deterministic = false;
+    int beta = 0;
+    bool pack = true;
+    int max_levels = 24;
+    int max_rounds = 32;
+    double stop = 0.90;
+    double growth = 2.0;
+};
+
+Opts to_opts(const gp_options* o) {
+    Opts r;
+    if (!o) return r;
+    r.parts = o->parts;
+    r.ratio = o->imbalance;
+    r.seed = o->seed;
+    r.verify = o->verify != 0;
+    r.deterministic = o->deterministic != 0;
+    r.beta = o->cluster_size_factor;
+    r.pack = o->pack_isolated != 0;
+    r.max_levels = o->max_levels;
+    r.max_rounds = o->max_rounds;
+    r.stop = o->stop_ratio;
+    r.growth = o->growth_ratio;
+    return r;
+}
+
+inline int production_beta(int parts) { return std::max(64, (512 + parts - 1) / parts); }
+
+template <typename T>
+struct Hierarchy {
+    std::vector<DGraph<T>> levels;
+    std::vector<Buf<i32>> maps;
+    std::string stop_reason = "capacity_floor";
+};
+
+template <typename T>
+void coarsen(Device& d, DGraph<T>&& input, const Opts& o, Hierarchy<T>& h, Log& log) {
+    const int beta = o.beta > 0 ? o.beta : production_beta(o.parts);
+    if (o.parts < 2 || o.parts > 32 || beta < 2 || o.max_levels < 0 || !std::isfinite(o.stop) || o.stop <= 0 || o.stop > 1)
+        fail(GP_EINVAL, "invalid coarsening options");
+    h.levels.clear();
+    h.maps.clear();
+    h.levels.reserve(static_cast<size_t>(o.max_levels) + 1);
+    const i64 cutoff = std::max<i64>(32, static_cast<i64>(beta) * o.parts);
+    DGraph<T> current = std::move(input);
+    SclpWork<T> work;
+    int level = 0;
+    for (; level < o.max_levels && current.n > cutoff; ++level) {
+        const u32 level_seed = o.seed + static_cast<u32>(level);
+        if (log.on)
+            log.out << "ml_coarsen_begin level=" << level << " vertices=" << current.n << " edges=" << current.m
+                    << " method=sclp seed=" << level_seed << '\n';
+        AggResult<T> agg;
+        aggregate(d, current, work, o.parts, level_seed, level, beta, o.pack, agg, log);
+        d.check_errors();
+        const double ratio = static_cast<double>(agg.coarse_n) / static_cast<double>(current.n);
+        if (agg.coarse_n >= current.n || ratio > o.stop) {
+            if (log.on) log.out << "ml_coarsen_stop reason=insufficient_contraction\n";
+            h.stop_reason = "insufficient_contraction";
+            break;
+        }
+        DGraph<T> coarse;
+        contract(d, current, agg.map.get(), agg.coarse_n, std::move(agg.cvw), coarse);
+        if (log.on)
+            log.out << "ml_gpu_contract_seconds level=" << level << " coarse_edges=" << coarse.m << '\n';
+        h.levels.push_back(std::move(current));
+        h.maps.push_back(std::move(agg.map));
+        current = std::move(coarse);
+    }
+    if (level == o.max_levels && current.n > cutoff) h.stop_reason = "max_levels";
+    h.levels.push_back(std::move(current));
+}
+
+// ---------------------------------------------------------------------------
+// Initial partition (src/initial_partition_gpu.cu:170-276)
+// ---------------------------------------------------------------------------
+struct DepthPlan {
+    std::vector<InitTask> tasks;   // first_part, parts, children filled; data fields by the device
+};
+
+std::vector<DepthPlan> plan_tasks(int parts) {
+    std::vector<DepthPlan> depths(1);
+    depths[0].tasks.push_back({0, 0, 0, parts, 0, -1, -1});
+    for (size_t dpt = 0; dpt < depths.size(); ++dpt) {
+        DepthPlan next;
+        for (auto& t : depths[dpt].tasks) {
+            const int lp = t.parts / 2, rp = t.parts - lp;
+            if (lp >= 2) { t.left_child = static_cast<i32>(next.tasks.size()); next.tasks.push_back({0, 0, t.first_part, lp, 0, -1, -1}); }
+            if (rp >= 2) { t.right_child = static_cast<i32>(next.tasks.size()); next.tasks.push_back({0, 0, t.first_part + lp, rp, 0, -1, -1}); }
+        }
+        if (!next.tasks.empty()) depths.push_back(std::move(next));
+    }
+    return depths;
+}
+
+template <typename T>
+void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask* tasks, const i32* task_of_pos,
+                      i32 positions, const i32* order, const i32* labels, u32 seed, int steps, float* deg, float* xa,
+                      float* xb, Moments* contrib, float* x_out, u64* key, u32* bar) {
+    using O = typename T::O;
+    using W = typename T::W;
+    auto kernel = diffusion_kernel<O, W>;
+    int per_sm = 0;
+    GP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+    const int max_grid = std::max(1, per_sm) * d.sms;
+    const int grid = std::max(1, std::min({max_grid, 2 * d.sms, blocks_for(positions, kWarps)}));
+    GP_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(u32), d.stream));
+    const O* off = g.off.get();
+    const i32* nbr = g.nbr.get();
+    const W* ew = g.ewp();
+    u32* bar_counter = bar;
+    u32* bar_gen = bar + 1;
+    u32* err = d.err;
+    void* args[] = {&ntasks, &tasks, &task_of_pos, &positions, &order, &labels, &off, &nbr, &ew, &seed, &steps,
+                    &deg, &xa, &xb, &contrib, &x_out, &key, &bar_counter, &bar_gen, &err};
+    cudaEvent_t ev0 = nullptr;
+    if (d.prof) { ev0 = d.event(); GP_CUDA(cudaEventRecord(ev0, d.stream)); }
+    GP_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kernel), grid, kThreads, args, 0, d.stream));
+    ++d.launches;
+    if (d.prof) {
+        cudaEvent_t ev1 = d.event();
+        GP_CUDA(cudaEventRecord(ev1, d.stream));
+        auto& e = d.prof_table["diffusion_kernel"];
+        e.pending.push_back({ev0, ev1});
+        ++e.launches;
+    }
+}
+
+template <typename T>
+void initial_partition(Device& d, const DGraph<T>& g, int parts, double ratio, u32 seed, Buf<i32>& labels,
+                       u64* initial_cut, Log& log) {
+    using W = typename T::W;
+    const i64 n64 = g.n;
+    if (n64 <= 0 || n64 > std::numeric_limits<int>::max() - 255 || parts < 2 || parts > n64 || parts > 32 ||
+        !std::isfinite(ratio) || ratio < 1.0)
+        fail(GP_EINVAL, "invalid GPU initial partition input");
+    const i32 n = static_cast<i32>(n64);
+    Buf<u64> sc(d, 8);
+    sc.zero(d);
+    launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, n), kThreads, 0, n, g.vwp(), sc.get());
+    launch(d, "sat_sum_kernel", sat_sum_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), sc.get() + 2);
+    GP_LAUNCH();
+    u64 st[3];
+    fetch(d, st, sc.get(), 3);
+    const u64 total = st[0], maxw = st[1], edge_total = st[2];
+    if (!total || total == ~0ULL || edge_total == ~0ULL)
+        fail(GP_EOVERFLOW, "GPU initializer weight accumulation overflow");
+    const u64 capacity = partition_capacity(total, parts, ratio);
+    if (maxw > capacity) fail(GP_EINVAL, "a vertex exceeds partition capacity");
+
+    labels = Buf<i32>(d, static_cast<size_t>(n));
+    labels.zero(d);
+    Buf<i32> order(d, static_cast<size_t>(n)), task_of_pos(d, static_cast<size_t>(n));
+    launch(d, "iota_kernel", iota_kernel, blocks_for(n, kThreads), kThreads, 0, n, order.get());
+    Buf<float> deg(d, static_cast<size_t>(n)), xa(d, static_cast<size_t>(n)), xb(d, static_cast<size_t>(n));
+    Buf<Moments> contrib(d, static_cast<size_t>(n));
+    Buf<u64> key(d, static_cast<size_t>(n)), key_alt(d, static_cast<size_t>(n)), prefix(d, static_cast<size_t>(n));
+    Buf<u32> bar(d, 2);
+    auto depths = plan_tasks(parts);
+    depths[0].tasks[0].count = n;
+    depths[0].tasks[0].weight = total;
+    std::vector<Buf<InitTask>> dtasks;
+    for (auto& dp : depths) {
+        dtasks.emplace_back(d, dp.tasks.size());
+        to_device(d, dtasks.back().get(), dp.tasks.data(), dp.tasks.size());
+    }
+    for (size_t dpt = 0; dpt < depths.size(); ++dpt) {
+        const int nt = static_cast<int>(depths[dpt].tasks.size());
+        GP_CUDA(cudaMemsetAsync(task_of_pos.get(), 0xff, n * sizeof(i32), d.stream));
+        launch(d, "task_positions_kernel", task_positions_kernel, nt, kThreads, 0, nt, dtasks[dpt].get(), task_of_pos.get());
+        GP_LAUNCH();
+        launch_diffusion(d, g, nt, dtasks[dpt].get(), task_of_pos.get(), n, order.get(), labels.get(), seed, 64,
+                         deg.get(), xa.get(), xb.get(), contrib.get(), nullptr, key.get(), bar.get());
+        launch(d, "task_sort_kernel", task_sort_kernel, nt, kThreads, 0, nt, dtasks[dpt].get(), key.get(), key_alt.get(), order.get());
+        InitTask* next = dpt + 1 < depths.size() ? dtasks[dpt + 1].get() : nullptr;
+        launch(d, "task_split_kernel", task_split_kernel<W>, nt, kThreads, 0, nt, dtasks[dpt].get(), next, order.get(), g.vwp(), capacity,
+                                                           prefix.get(), labels.get(), d.err);
+        GP_LAUNCH();
+    }
+    d.check_errors();
+    Buf<u64> loads(d, static_cast<size_t>(parts) + 1);
+    loads.zero(d);
+    launch(d, "part_weight_kernel", part_weight_kernel<W>, blocks_for(n, kThreads), kThreads, 0, n, labels.get(), g.vwp(), loads.get());
+    launch(d, "cut_kernel", cut_kernel<typename T::O, W>, stride_grid(d, static_cast<i64>(n) * 32), kThreads, 0, 
+        n, g.off.get(), g.nbr.get(), g.ewp(), labels.get(), loads.get() + parts);
+    GP_LAUNCH();
+    std::vector<u64> host(static_cast<size_t>(parts) + 1);
+    fetch(d, host.data(), loads.get(), host.size());
+    if (*std::max_element(host.begin(), host.begin() + parts) > capacity)
+        fail(GP_ERUNTIME, "GPU initializer balance validation failed");
+    if (initial_cut) *initial_cut = host[parts] / 2;
+    if (log.on)
+        log.out << "initial_partition_backend=gpu_spectral_batched_fp32\ncoarsest_vertices=" << n
+                << "\ncoarsest_edge_entries=" << g.m << "\ninitial_partition_parts=" << parts
+                << "\ninitial_partition_edgecut=" << host[parts] / 2 << '\n';
+}
+
+// ---------------------------------------------------------------------------
+// Refinement (src/refine_incremental.cuh:235-361, src/refine.cu:423-646)
+// ---------------------------------------------------------------------------
+struct BucketThresholdsHost {
+    BucketThresholds t;
+    BucketThresholdsHost() { for (int j = -23; j <= 24; ++j) t.t[j + 23] = std::pow(1.5, j); }
+};
+
+template <typename T>
+u64 directed_cut(Device& d, const DGraph<T>& g, const i32* labels, u64* scratch) {
+    GP_CUDA(cudaMemsetAsync(scratch, 0, sizeof(u64), d.stream));
+    d.prof_bytes("cut_kernel", static_cast<double>(g.n + 1) * sizeof(typename T::O) + g.n * 4.0 +
+                                   static_cast<double>(g.m) * (4 + 4 + (g.ewp() ? sizeof(typename T::W) : 0)));
+    launch(d, "cut_kernel", cut_kernel<typename T::O, typename T::W>, stride_grid(d, g.n * 32), kThreads, 0, 
+        g.n, g.off.get(), g.nbr.get(), g.ewp(), labels, scratch);
+    GP_LAUNCH();
+    u64 c = 0;
+    fetch(d, &c, scratch, 1);
+    return c;
+}
+
+template <typename T>
+u64 undirected_cut(Device& d, const DGraph<T>& g, const i32* labels, u64* scratch) {
+    const u64 c = directed_cut(d, g, labels, scratch);
+    if (c & 1ULL) fail(GP_ERUNTIME, "refinement cut is not symmetric");
+    return c / 2;
+}
+
+struct RefineWork {
+    Buf<unsigned char> cache_raw;
+    Buf<i32> targets, list, movers, saved_labels, clist, clist_alt;
+    Buf<i64> gains, pos;
+    Buf<unsigned char> locks, flags;
+    Buf<double> gpw;
+    Buf<i32> bucket;
+    Buf<u64> rank, counts, offsets, saved_pw, excl, keys, keys_alt, bucket_base, scratch;
+    Buf<RefineCounters> ctr;
+    void ensure(Device& d, i64 n, int k, size_t cache_bytes) {
+        const size_t s = static_cast<size_t>(n) + 1;
+        cache_raw.ensure(d, cache_bytes);
+        targets.ensure(d, s); list.ensure(d, s); movers.ensure(d, s); saved_labels.ensure(d, s);
+        clist.ensure(d, s); clist_alt.ensure(d, s);
+        gains.ensure(d, s); pos.ensure(d, s);
+        locks.ensure(d, s); flags.ensure(d, s);
+        gpw.ensure(d, s); bucket.ensure(d, s);
+        rank.ensure(d, s); excl.ensure(d, s); keys.ensure(d, s); keys_alt.ensure(d, s);
+        counts.ensure(d, static_cast<size_t>(k) * kBalWidth);
+        offsets.ensure(d, static_cast<size_t>(k) * kBalWidth);
+        bucket_base.ensure(d, static_cast<size_t>(k) * kBalWidth);
+        saved_pw.ensure(d, 32);
+        scratch.ensure(d, 8);
+        ctr.ensure(d, 1);
+    }
+};
+
+template <typename T, typename C>
+gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* labels, u64* pw,
+                             std::vector<u64>& host_pw, int k, u64 cap, int rounds, bool deterministic, bool verify) {
+    using O = typename T::O;
+    using W = typename T::W;
+    const i64 n = g.n;
+    w.ensure(d, n, k, static_cast<size_t>(n) * k * sizeof(C));
+    C* cache = reinterpret_cast<C*>(w.cache_raw.get());
+    const O* off = g.off.get();
+    const i32* nbr = g.nbr.get();
+    const W* ew = g.ewp();
+    const W* vw = g.vwp();
+    RefineCounters* ctr = w.ctr.get();
+    static const BucketThresholdsHost thresholds;
+    gp_refine_stats st{};
+    w.locks.zero(d);
+    w.flags.zero(d);
+    d.prof_bytes("build_cache_kernel", static_cast<double>(n + 1) * sizeof(O) +
+                                           static_cast<double>(g.m) * (4 + 4 + (ew ? sizeof(W) : 0)) +
+                                           static_cast<double>(n) * k * sizeof(C));
+    launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr, ew, labels, k, cache);
+    GP_LAUNCH();
+    u64 current_cut = undirected_cut(d, g, labels, w.scratch.get());
+    st.initial_cut = current_cut;
+    u64 best_cut = current_cut;
+    auto checkpoint = [&]() {
+        GP_CUDA(cudaMemcpyAsync(w.saved_labels.get(), labels, n * sizeof(i32), cudaMemcpyDeviceToDevice, d.stream));
+        GP_CUDA(cudaMemcpyAsync(w.saved_pw.get(), pw, k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
+    };
+    checkpoint();
+    auto maximum = [&]() { return *std::max_element(host_pw.begin(), host_pw.end()); };
+    // maximum edge weight decides the LP filter (refine_incremental.cuh:332-333)
+    u64 maxe = 1;
+    if (ew) {
+        GP_CUDA(cudaMemsetAsync(w.scratch.get(), 0, sizeof(u64), d.stream));
+        launch(d, "max_weight_kernel", max_weight_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, ew, w.scratch.get());
+        GP_LAUNCH();
+        fetch(d, &maxe, w.scratch.get(), 1);
+    } else if (g.m == 0) {
+        maxe = 0;
+    }
+    const double filter = maxe <= 1 ? 0.25 : 0.75;
+    struct Stats { RefineCounters c; u64 pw[32]; };
+    Buf<Stats> stats_dev(d, 1);
+    auto finish_apply = [&](bool lp) -> i64 {
+        // movers already listed in w.movers with counter ctr->movers
+        launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, 
+            w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
+        launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, n), kThreads, 0, w.movers.get(), ctr, labels, w.targets.get(), vw,
+                                                                      pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
+        GP_LAUNCH();
+        GP_CUDA(cudaMemcpyAsync(&stats_dev.get()->c, ctr, sizeof(RefineCounters), cudaMemcpyDeviceToDevice, d.stream));
+        GP_CUDA(cudaMemcpyAsync(stats_dev.get()->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
+        Stats h;
+        fetch(d, &h, stats_dev.get(), 1);
+        const long long delta = h.c.delta;
+        if (delta >= 0) {
+            if (static_cast<u64>(delta) > current_cut) fail(GP_ERUNTIME, "incremental cut underflow");
+            current_cut -= static_cast<u64>(delta);
+        } else {
+            current_cut += static_cast<u64>(-delta);
+        }
+        std::copy(h.pw, h.pw + k, host_pw.begin());
+        st.accepted += static_cast<u64>(h.c.movers);
+        if (verify) {
+            const u64 recount = undirected_cut(d, g, labels, w.scratch.get());
+            if (recount != current_cut) fail(GP_ERUNTIME, "incremental cut differs from CSR scan");
+        }
+        return h.c.movers;
+    };
+    auto deterministic_ranks = [&]() {
+        // candidates in ascending vertex order, sorted by (bucket, gpw desc)
+        exclusive_scan<i64>(d, HasBucket{w.bucket.get()}, w.pos.get(), n, reinterpret_cast<i64*>(w.scratch.get() + 1));
+        launch(d, "compact_bucket_kernel", compact_bucket_kernel, blocks_for(n, kThreads), kThreads, 0, n, w.bucket.get(), w.pos.get(),
+                                                                                  w.clist.get());
+        GP_LAUNCH();
+        i64 count = 0;
+        fetch(d, &count, reinterpret_cast<i64*>(w.scratch.get() + 1), 1);
+        w.counts.zero(d);
+        if (count == 0) return;
+        launch(d, "rank_keys_kernel", rank_keys_kernel, blocks_for(count, kThreads), kThreads, 0, count, w.clist.get(), w.gpw.get(),
+                                                                                w.bucket.get(), 0, w.keys.get());
+        GP_LAUNCH();
+        radix_sort<u64, i32>(d, w.keys.get(), w.clist.get(), w.keys_alt.get(), w.clist_alt.get(), count, 0, 64);
+        launch(d, "rank_keys_kernel", rank_keys_kernel, blocks_for(count, kThreads), kThreads, 0, count, w.clist.get(), w.gpw.get(),
+                                                                                w.bucket.get(), 1, w.keys.get());
+        GP_LAUNCH();
+        radix_sort<u64, i32>(d, w.keys.get(), w.clist.get(), w.keys_alt.get(), w.clist_alt.get(), count, 0,
+                             std::max(1, bit_width_u64(static_cast<u64>(k) * kBalWidth)));
+        exclusive_scan<u64>(d, ListWeight<W>{w.clist.get(), vw}, w.excl.get(), count);
+        launch(d, "bucket_heads_kernel", bucket_heads_kernel, blocks_for(count, kThreads), kThreads, 0, count, w.clist.get(), w.bucket.get(),
+                                                                                   w.excl.get(), w.bucket_base.get());
+        launch(d, "bucket_ranks_kernel", bucket_ranks_kernel<W>, blocks_for(count, kThreads), kThreads, 0, 
+            count, w.clist.get(), w.bucket.get(), w.excl.get(), w.bucket_base.get(), vw, w.rank.get(), w.counts.get());
+        GP_LAUNCH();
+    };
+    auto rebalance = [&]() -> bool {
+        for (int it = 0; it < 2 * k + 4 && maximum() > cap; ++it) {
+            ++st.admission_iterations;
+            GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
+            w.counts.zero(d);
+            launch(d, "rebalance_proposals_kernel", rebalance_proposals_kernel<C, W>, blocks_for(n, kThreads), kThreads, 0, 
+                n, cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(), w.gpw.get(),
+                w.bucket.get(), w.rank.get(), w.counts.get());
+            GP_LAUNCH();
+            if (deterministic) deterministic_ranks();
+            launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
+            w.counts.zero(d);
+            launch(d, "select_sources_kernel", select_sources_kernel<W>, blocks_for(n, kThreads), kThreads, 0, 
+                n, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, w.targets.get(), vw, deterministic ? 1 : 0,
+                w.counts.get());
+            GP_LAUNCH();
+            if (deterministic) deterministic_ranks();
+            launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
+            launch(d, "select_destinations_kernel", select_destinations_kernel<W>, blocks_for(n, kThreads), kThreads, 0, 
+                n, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(), w.movers.get(), ctr);
+            GP_LAUNCH();
+            const i64 moved = finish_apply(false);
+            if (!moved) return false;
+        }
+        return maximum() <= cap;
+    };
+    int stale = 0, empty = 0;
+    for (int phase = 0; phase < rounds && stale < 3; ++phase) {
+        st.rounds = phase + 1;
+        GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
+        d.prof_bytes("lp_proposals_kernel", static_cast<double>(n) * (k * sizeof(C) + 4 + 1 + 4 + 8));
+        launch(d, "lp_proposals_kernel", lp_proposals_kernel<C>, blocks_for(n, kThreads), kThreads, 0, 
+            n, cache, labels, k, filter, w.locks.get(), w.targets.get(), w.gains.get(), w.list.get(), ctr);
+        launch(d, "priority_filter_kernel", priority_filter_kernel<O, W>, stride_grid(d, n * 32), kThreads, 0, 
+            w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.gains.get(), w.flags.get(), w.movers.get(), ctr);
+        GP_LAUNCH();
+        const i64 count = finish_apply(true);
+        st.proposals += static_cast<u64>(count);
+        if (!count) {
+            if (++empty >= 2) break;
+            ++stale;
+            continue;
+        }
+        empty = 0;
+        if (!rebalance()) { ++st.admission_fallbacks; break; }
+        ++stale;
+        if (current_cut < best_cut) {
+            if (static_cast<long double>(current_cut) < 0.999L * best_cut) stale = 0;
+            best_cut = current_cut;
+            checkpoint();
+        }
+    }
+    GP_CUDA(cudaMemcpyAsync(labels, w.saved_labels.get(), n * sizeof(i32), cudaMemcpyDeviceToDevice, d.stream));
+    GP_CUDA(cudaMemcpyAsync(pw, w.saved_pw.get(), k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
+    fetch(d, host_pw.data(), pw, static_cast<size_t>(k));
+    st.final_cut = undirected_cut(d, g, labels, w.scratch.get());
+    st.final_max_part_weight = maximum();
+    if (st.final_cut != best_cut || st.final_cut > st.initial_cut || maximum() > cap)
+        fail(GP_ERUNTIME, "incremental refinement postcondition failed");
+    return st;
+}
+
+template <typename T>
+bool narrow_cache(const DGraph<T>& g, Device& d) {
+    if constexpr (sizeof(typename T::W) == 8) {
+        (void)g; (void)d;
+        return false;
+    } else {
+        Buf<u64> s(d, 1);
+        s.zero(d);
+        launch(d, "sat_sum_kernel", sat_sum_kernel<typename T::W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), s.get());
+        GP_LAUNCH();
+        u64 total = 0;
+        fetch(d, &total, s.get(), 1);
+        return total <= 0xffffffffULL;
+    }
+}
+
+template <typename T>
+gp_refine_stats refine_dispatch(Device& d, const DGraph<T>& g, RefineWork& w, i32* labels, u64* pw,
+                                std::vector<u64>& host_pw, int k, u64 cap, int rounds, bool det, bool verify, bool narrow) {
+    // validate_refinement_gain_range (src/refine.cu:346-383): only the big
+    // width can exceed INT64_MAX/2 in total directed weight.
+    if constexpr (sizeof(typename T::W) == 8) {
+        Buf<u64> s(d, 1);
+        s.zero(d);
+        launch(d, "sat_sum_kernel", sat_sum_kernel<typename T::W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), s.get());
+        GP_LAUNCH();
+        u64 total = 0;
+        fetch(d, &total, s.get(), 1);
+        if (total > static_cast<u64>(INT64_MAX) / 2) fail(GP_EOVERFLOW, "refinement signed gain range exceeded");
+    }
+    if (narrow) return refine_level<T, u32>(d, g, w, labels, pw, host_pw, k, cap, rounds, det, verify);
+    return refine_level<T, u64>(d, g, w, labels, pw, host_pw, k, cap, rounds, det, verify);
+}
+
+template <typename T>
+void part_weights(Device& d, const DGraph<T>& g, const i32* labels, int k, u64* pw, std::vector<u64>& host) {
+    GP_CUDA(cudaMemsetAsync(pw, 0, k * sizeof(u64), d.stream));
+    launch(d, "part_weight_kernel", part_weight_kernel<typename T::W>, blocks_for(g.n, kThreads), kThreads, 0, g.n, labels, g.vwp(), pw);
+    GP_LAUNCH();
+    host.assign(static_cast<size_t>(k), 0);
+    fetch(d, host.data(), pw, static_cast<size_t>(k));
+}
+
+struct UncoarsenResult {
+    u64 cut = 0;
+    u64 total_edge_weight = 0;
+    std::vector<u64> pw;
+};
+
+// refine_hierarchy_impl (src/refine.cu:423-646) + uncoarsen_impl's report
+// (src/uncoarsen.cu:39-97).  Consumes the hierarchy's levels.
+template <typename T>
+void uncoarsen(Device& d, Hierarchy<T>& h, Buf<i32>& labels, const Opts& o, u64 cap, UncoarsenResult& r, Log& log) {
+    const int k = o.parts;
+    RefineWork work;
+    Buf<u64> pw(d, 32);
+    std::vector<u64> host_pw;
+    auto& coarsest = h.levels.back();
+    const bool narrow = narrow_cache(coarsest, d) && narrow_cache(h.levels.front(), d);
+    part_weights(d, coarsest, labels.get(), k, pw.get(), host_pw);
+    if (*std::max_element(host_pw.begin(), host_pw.end()) > cap)
+        fail(GP_EINVAL, "initial refinement partition is imbalanced");
+    auto st = refine_dispatch(d, coarsest, work, labels.get(), pw.get(), host_pw, k, cap, o.max_rounds,
+                              o.deterministic, o.verify, narrow);
+    u64 last_cut = st.final_cut;
+    i64 last_refined = coarsest.n;
+    if (log.on)
+        log.out << "refine_coarsest vertices=" << coarsest.n << " initial_cut=" << st.initial_cut
+                << " final_cut=" << st.final_cut << " rounds=" << st.rounds << '\n';
+    for (size_t lv = h.levels.size() - 1; lv > 0; --lv) {
+        const size_t fine_level = lv - 1;
+        auto& fine = h.levels[fine_level];
+        Buf<i32> fine_labels(d, static_cast<size_t>(fine.n));
+        launch(d, "project_kernel", project_kernel, blocks_for(fine.n, kThreads), kThreads, 0, fine.n, h.maps[fine_level].get(),
+                                                                                labels.get(), fine_labels.get());
+        GP_LAUNCH();
+        labels = std::move(fine_labels);
+        h.levels.pop_back();
+        h.maps.pop_back();
+        if (o.verify) {
+            std::vector<u64> check;
+            Buf<u64> pw2(d, 32);
+            part_weights(d, fine, labels.get(), k, pw2.get(), check);
+            const u64 c = undirected_cut(d, fine, labels.get(), work.scratch.get());
+            if (c != last_cut || check != host_pw)
+                fail(GP_ERUNTIME, "GPU projection failed cut or part-weight preservation");
+        }
+        const bool refine_this = fine_level == 0 || static_cast<double>(fine.n) >= o.growth * static_cast<double>(last_refined);
+        gp_refine_stats ls{};
+        if (refine_this) {
+            ls = refine_dispatch(d, fine, work, labels.get(), pw.get(), host_pw, k, cap, o.max_rounds,
+                                 o.deterministic, o.verify, narrow);
+            last_refined = fine.n;
+        } else {
+            ls.initial_cut = ls.final_cut = last_cut;
+            ls.final_max_part_weight = *std::max_element(host_pw.begin(), host_pw.end());
+        }
+        last_cut = ls.final_cut;
+        if (log.on)
+            log.out << "uncoarsen_level=" << fine_level << " vertices=" << fine.n << " edge_entries=" << fine.m
+                    << " projection_cut=" << ls.initial_cut << " refine_rounds=" << ls.rounds
+                    << " refine_proposals=" << ls.proposals << " refine_accepted=" << ls.accepted
+                    << " admission_iterations=" << ls.admission_iterations
+                    << " admission_fallbacks=" << ls.admission_fallbacks << " refined_cut=" << ls.final_cut
+                    << " refined_max_part_weight=" << ls.final_max_part_weight << '\n';
+    }
+    auto& finest = h.levels.front();
+    u64 directed = 0;
+    if (finest.ewp()) {
+        Buf<u64> s(d, 1);
+        s.zero(d);
+        launch(d, "sum_weight_kernel", sum_weight_kernel<typename T::W>, stride_grid(d, finest.m), kThreads, 0, finest.m, finest.ewp(), s.get());
+        GP_LAUNCH();
+        fetch(d, &directed, s.get(), 1);
+    } else {
+        directed = static_cast<u64>(finest.m);
+    }
+    if (directed & 1ULL) fail(GP_ERUNTIME, "symmetric graph has odd directed edge weight");
+    r.cut = last_cut;
+    r.total_edge_weight = directed / 2;
+    r.pw = host_pw;
+}
+
+// ---------------------------------------------------------------------------
+// Input preparation: upload, narrowing and validation on the GPU with the
+// rules and messages of src/graph.cpp:47-190.
+// ---------------------------------------------------------------------------
+template <typename O>
+__global__ void narrow_offsets_kernel(i64 n, const i64* in, O* out, i64 m, u32* err) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const i64 x = in[i];
+    if (x < 0 || x > m || (i > 0 && x < in[i - 1])) set_error(err, kErrBadInput);
+    out[i] = static_cast<O>(x);
+}
+
+__global__ void narrow_neighbors_kernel(i64 m, const i64* in, i32* out, i64 n, u32* err) {
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 x = in[i];
+        if (x < 0 || x >= n) set_error(err, kErrBadInput);
+        out[i] = static_cast<i32>(x);
+    }
+}
+
+template <typename O>
+__global__ void check_offsets_kernel(i64 n, const O* off, i64 m, u32* err) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const i64 x = static_cast<i64>(off[i]);
+    if (x < 0 || x > m || (i > 0 && x < static_cast<i64>(off[i - 1])) || (i == 0 && x != 0) || (i == n && x != m))
+        set_error(err, kErrBadInput);
+}
+
+__global__ void check_neighbors_kernel(i64 m, const i32* nbr, i64 n, u32* err) {
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        if (nbr[i] < 0 || nbr[i] >= n) set_error(err, kErrBadInput);
+}
+
+// --verify: every entry (v,u,w) has a reverse entry (u,v,w) found by binary
+// search in u's row (validate_weighted_csr, src/graph.cpp:164-190).
+template <typename O, typename W>
+__global__ void symmetry_kernel(i64 n, const O* off, const i32* nbr, const W* ew, u32* err) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    for (i64 e = off[v]; e < static_cast<i64>(off[v + 1]); ++e) {
+        const i32 u = nbr[e];
+        i64 lo = off[u], hi = off[u + 1];
+        while (lo < hi) {
+            const i64 mid = lo + (hi - lo) / 2;
+            if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+        }
+        if (lo == static_cast<i64>(off[u + 1]) || nbr[lo] != v || weight_at(ew, e) != weight_at(ew, lo)) {
+            set_error(err, kErrOddCut);
+            return;
+        }
+    }
+}
+
+template <typename T>
+void prepare_graph(Device& d, const gp_graph* gi, DGraph<T>& g, bool verify) {
+    using O = typename T::O;
+    using W = typename T::W;
+    if (!gi) fail(GP_EINVAL, "null graph");
+    const i64 n = gi->n, m = gi->m;
+    if (n < 0 || m < 0) fail(GP_EINVAL, "invalid graph size");
+    if constexpr (std::is_same_v<T, Std>) {
+        if (n > std::numeric_limits<i32>::max() || m > std::numeric_limits<i32>::max())
+            fail(GP_ERUNTIME, "graph exceeds standard CSR limits; use gpart_coarsen_big");
+    } else if (n > std::numeric_limits<i32>::max()) {
+        fail(GP_ERUNTIME, "graph vertex ids exceed configured graph type");
+    }
+    const bool on_dev = gi->memory == GP_MEMORY_DEVICE;
+    const cudaMemcpyKind kind = on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    g.n = n;
+    g.m = m;
+    // Device input in the width's own types is used in place (borrowed):
+    // a resident graph is partitioned without a copy.
+    const bool borrow = on_dev && !gi->index64;
+    if (borrow) {
+        g.off.borrow(static_cast<O*>(const_cast<void*>(gi->offsets)), static_cast<size_t>(n) + 1);
+        g.nbr.borrow(static_cast<i32*>(const_cast<void*>(gi->neighbors)), static_cast<size_t>(m));
+    } else {
+        g.off = Buf<O>(d, static_cast<size_t>(n) + 1);
+        g.nbr = Buf<i32>(d, static_cast<size_t>(std::max<i64>(m, 1)));
+    }
+    if (borrow) {
+    } else if (gi->index64) {
+        Buf<i64> tmp(d, static_cast<size_t>(std::max<i64>(n + 1, m)));
+        GP_CUDA(cudaMemcpyAsync(tmp.get(), gi->offsets, (n + 1) * sizeof(i64), kind, d.stream));
+        launch(d, "narrow_offsets_kernel", narrow_offsets_kernel<O>, blocks_for(n + 1, kThreads), kThreads, 0, n, tmp.get(), g.off.get(), m, d.err);
+        GP_LAUNCH();
+        if (m) {
+            GP_CUDA(cudaMemcpyAsync(tmp.get(), gi->neighbors, m * sizeof(i64), kind, d.stream));
+            launch(d, "narrow_neighbors_kernel", narrow_neighbors_kernel, stride_grid(d, m), kThreads, 0, m, tmp.get(), g.nbr.get(), n, d.err);
+            GP_LAUNCH();
+        }
+    } else {
+        GP_CUDA(cudaMemcpyAsync(g.off.get(), gi->offsets, (n + 1) * sizeof(O), kind, d.stream));
+        if (m) GP_CUDA(cudaMemcpyAsync(g.nbr.get(), gi->neighbors, m * sizeof(i32), kind, d.stream));
+    }
+    launch(d, "check_offsets_kernel", check_offsets_kernel<O>, blocks_for(n + 1, kThreads), kThreads, 0, n, g.off.get(), m, d.err);
+    if (!gi->index64 && m) launch(d, "check_neighbors_kernel", check_neighbors_kernel, stride_grid(d, m), kThreads, 0, m, g.nbr.get(), n, d.err);
+    GP_LAUNCH();
+    g.unit_ew = gi->edge_weights == nullptr;
+    g.unit_vw = gi->vertex_weights == nullptr;
+    if (!g.unit_ew) {
+        if (on_dev) {
+            g.ew.borrow(static_cast<W*>(const_cast<void*>(gi->edge_weights)), static_cast<size_t>(m));
+        } else {
+            g.ew = Buf<W>(d, static_cast<size_t>(std::max<i64>(m, 1)));
+            if (m) GP_CUDA(cudaMemcpyAsync(g.ew.get(), gi->edge_weights, m * sizeof(W), kind, d.stream));
+        }
+    }
+    if (!g.unit_vw) {
+        if (on_dev) {
+            g.vw.borrow(static_cast<W*>(const_cast<void*>(gi->vertex_weights)), static_cast<size_t>(n));
+        } else {
+            g.vw = Buf<W>(d, static_cast<size_t>(std::max<i64>(n, 1)));
+            if (n) GP_CUDA(cudaMemcpyAsync(g.vw.get(), gi->vertex_weights, n * sizeof(W), kind, d.stream));
+        }
+    }
+    if (verify && n)
+        launch(d, "symmetry_kernel", symmetry_kernel<O, W>, blocks_for(n, kThreads), kThreads, 0, n, g.off.get(), g.nbr.get(), g.ewp(), d.err);
+    GP_LAUNCH();
+    u32 e = 0;
+    fetch(d, &e, d.err, 1);
+    if (e) {
+        GP_CUDA(cudaMemsetAsync(d.err, 0, sizeof(u32), d.stream));
+        if (e & kErrOddCut) fail(GP_ERUNTIME, "weighted CSR is not bidirectional");
+        fail(GP_ERUNTIME, "weighted CSR shape is invalid (offsets not monotone or neighbor out of range)");
+    }
+}
+
+template <typename T>
+void host_level_copy(Device& d, const DGraph<T>& g, const i32* map, i64 map_n, std::vector<i64>& off,
+                     std::vector<i32>& nbr, std::vector<u64>& ew, std::vector<u64>& vw, std::vector<i32>& mp) {
+    using O = typename T::O;
+    using W = typename T::W;
+    std::vector<O> o(static_cast<size_t>(g.n) + 1);
+    to_host(d, o.data(), g.off.get(), o.size());
+    nbr.resize(static_cast<size_t>(g.m));
+    to_host(d, nbr.data(), g.nbr.get(), nbr.size());
+    std::vector<W> e, v;
+    if (g.ewp()) { e.resize(static_cast<size_t>(g.m)); to_host(d, e.data(), g.ewp(), e.size()); }
+    if (g.vwp()) { v.resize(static_cast<size_t>(g.n)); to_host(d, v.data(), g.vwp(), v.size()); }
+    mp.resize(static_cast<size_t>(map ? map_n : 0));
+    if (map) to_host(d, mp.data(), map, mp.size());
+    d.sync();
+    off.assign(o.begin(), o.end());
+    ew.resize(static_cast<size_t>(g.m));
+    vw.resize(static_cast<size_t>(g.n));
+    for (i64 i = 0; i < g.m; ++i) ew[i] = g.ewp() ? static_cast<u64>(e[i]) : 1;
+    for (i64 i = 0; i < g.n; ++i) vw[i] = g.vwp() ? static_cast<u64>(v[i]) : 1;
+}
+
+}  // namespace gp
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct gp_ctx {
+    gp::Device dev;
+    std::string error;
+};
+
+struct gp_hierarchy {
+    struct Level {
+        std::vector<int64_t> off;
+        std::vector<int32_t> nbr;
+        std::vector<uint64_t> ew, vw;
+        std::vector<int32_t> map;   // to the next level
+    };
+    std::vector<Level> levels;
+    std::string stop_reason;
+};
+
+namespace {
+
+template <typename F>
+gp_status guarded(gp_ctx* ctx, F&& f) {
+    try {
+        f();
+        if (ctx) ctx->error.clear();
+        return GP_OK;
+    } catch (const gp::Error& e) {
+        if (ctx) ctx->error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->error = "host allocation failed";
+        return GP_ENOMEM;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->error = e.what();
+        return GP_ERUNTIME;
+    }
+}
+
+template <typename F>
+void with_width(const gp_graph* g, F&& f) {
+    if (!g) gp::fail(GP_EINVAL, "null graph");
+    if (g->width == GP_WIDTH_BIG) f(gp::Big{});
+    else if (g->width == GP_WIDTH_STANDARD) f(gp::Std{});
+    else gp::fail(GP_EINVAL, "invalid graph width");
+}
+
+}  // namespace
+
+extern "C" {
+
+void gp_options_default(gp_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->parts = 4;
+    o->cluster_size_factor = 0;
+    o->imbalance = 1.03;
+    o->seed = 0;
+    o->pack_isolated = 1;
+    o->max_levels = 24;
+    o->max_rounds = 32;
+    o->stop_ratio = 0.90;
+    o->growth_ratio = 2.0;
+}
+
+gp_status gp_ctx_create(int device, gp_ctx** out) {
+    if (!out) return GP_EINVAL;
+    auto ctx = std::make_unique<gp_ctx>();
+    const gp_status s = guarded(ctx.get(), [&] {
+        auto& d = ctx->dev;
+        d.device = device;
+        GP_CUDA(cudaSetDevice(device));
+        GP_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
+        GP_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        GP_CUDA(cudaMemPoolCreate(&d.pool, &props));
+        gp::u64 keep = UINT64_MAX;
+        GP_CUDA(cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        GP_CUDA(cudaMalloc(&d.err, 64));
+        GP_CUDA(cudaMemset(d.err, 0, 64));
+        GP_CUDA(cudaMallocHost(&d.pinned, gp::Device::kPinnedBytes));
+    });
+    if (s != GP_OK) {
+        *out = nullptr;
+        return s;
+    }
+    *out = ctx.release();
+    return GP_OK;
+}
+
+void gp_ctx_destroy(gp_ctx* ctx) {
+    if (!ctx) return;
+    auto& d = ctx->dev;
+    cudaSetDevice(d.device);
+    if (d.stream) cudaStreamSynchronize(d.stream);
+    if (d.err) cudaFree(d.err);
+    if (d.pinned) cudaFreeHost(d.pinned);
+    if (d.pool) cudaMemPoolDestroy(d.pool);
+    if (d.stream) cudaStreamDestroy(d.stream);
+    delete ctx;
+}
+
+const char* gp_ctx_error(const gp_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+gp_status gp_partition_capacity(uint64_t total, int parts, double ratio, uint64_t* out) {
+    return guarded(nullptr, [&] { *out = gp::partition_capacity(total, parts, ratio); });
+}
+
+gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* options, int32_t* labels,
+                       gp_report* report) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        const gp::Opts o = gp::to_opts(options);
+        gp::Log log;
+        log.on = options && options->log;
+        gp_report rep{};
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            rep.n = graph->n;
+            rep.m = graph->m;
+            gp::partition_capacity(static_cast<gp::u64>(graph->n), o.parts, o.ratio);
+            const auto prep_start = gp::Clock::now();
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, o.verify);
+            d.sync();
+            rep.prepare_seconds = gp::seconds_since(prep_start);
+            // algorithm_total_seconds scope (app/partition_main.cu:67-93)
+            const auto t0 = gp::Clock::now();
+            gp::u64 total = 0;
+            {
+                gp::Buf<gp::u64> s(d, 2);
+                s.zero(d);
+                launch(d, "weight_stats_kernel", gp::weight_stats_kernel<typename T::W>, gp::stride_grid(d, g.n), gp::kThreads, 0, 
+                    g.n, g.vwp(), s.get());
+                GP_LAUNCH();
+                gp::fetch(d, &total, s.get(), 1);
+            }
+            const gp::u64 cap = gp::partition_capacity(total, o.parts, o.ratio);
+            gp::Hierarchy<T> h;
+            gp::coarsen<T>(d, std::move(g), o, h, log);
+            d.sync();
+            const auto t1 = gp::Clock::now();
+            rep.levels = static_cast<int32_t>(h.levels.size());
+            rep.coarsest_n = h.levels.back().n;
+            gp::Buf<gp::i32> lab;
+            gp::initial_partition<T>(d, h.levels.back(), o.parts, o.ratio, o.seed, lab, &rep.initial_cut, log);
+            d.sync();
+            const auto t2 = gp::Clock::now();
+            gp::UncoarsenResult ur;
+            gp::uncoarsen<T>(d, h, lab, o, cap, ur, log);
+            d.sync();
+            const auto t3 = gp::Clock::now();
+            h.levels.clear();
+            h.maps.clear();
+            d.sync();
+            const auto t4 = gp::Clock::now();
+            rep.coarsen_seconds = std::chrono::duration<double>(t1 - t0).count();
+            rep.initial_seconds = std::chrono::duration<double>(t2 - t1).count();
+            rep.uncoarsen_seconds = std::chrono::duration<double>(t3 - t2).count();
+            rep.free_seconds = std::chrono::duration<double>(t4 - t3).count();
+            rep.algorithm_seconds = std::chrono::duration<double>(t4 - t0).count();
+            rep.cut = ur.cut;
+            rep.capacity = cap;
+            rep.total_edge_weight = ur.total_edge_weight;
+            for (size_t i = 0; i < ur.pw.size() && i < 32; ++i) rep.part_weights[i] = ur.pw[i];
+            if (labels) {
+                const bool dev_out = graph->memory == GP_MEMORY_DEVICE;
+                GP_CUDA(cudaMemcpyAsync(labels, lab.get(), graph->n * sizeof(int32_t),
+                                        dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, d.stream));
+            }
+            lab.reset();
+            d.sync();
+            if (log.on) {
+                const gp::u64 mx = ur.pw.empty() ? 0 : *std::max_element(ur.pw.begin(), ur.pw.end());
+                std::cout << std::setprecision(10) << "final_edge_cut=" << ur.cut << '\n'
+                          << "final_cut_ratio="
+                          << (ur.total_edge_weight == 0 ? 0.0 : static_cast<double>(ur.cut) / ur.total_edge_weight)
+                          << '\n'
+                          << "final_max_part_weight=" << mx << '\n'
+                          << "final_imbalance="
+                          << (total == 0 ? 0.0 : static_cast<double>(mx) * o.parts / static_cast<double>(total)) << '\n';
+            }
+        });
+        if (report) *report = rep;
+    });
+}
+
+gp_status gp_aggregate(gp_ctx* ctx, const gp_graph* graph, int parts, uint32_t seed, int level,
+                       int cluster_size_factor, int pack_isolated, int32_t* map, int64_t* coarse_n,
+                       uint64_t* cluster_cap) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            gp::SclpWork<T> w;
+            gp::AggResult<T> r;
+            gp::Log log;
+            gp::aggregate<T>(d, g, w, parts, seed, level, cluster_size_factor, pack_isolated != 0, r, log);
+            d.check_errors();
+            if (map) gp::to_host(d, map, r.map.get(), static_cast<size_t>(g.n));
+            d.sync();
+            if (coarse_n) *coarse_n = r.coarse_n;
+            if (cluster_cap) *cluster_cap = r.cap;
+        });
+    });
+}
+
+gp_status gp_contract(gp_ctx* ctx, const gp_graph* graph, const int32_t* map, int64_t coarse_n, int64_t* offsets,
+                      int32_t* neighbors, uint64_t* edge_weights, uint64_t* vertex_weights, int64_t* coarse_m) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            using W = typename T::W;
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            if (coarse_n <= 0 || coarse_n > g.n) gp::fail(GP_EINVAL, "invalid coarse vertex count");
+            gp::Buf<gp::i32> dmap(d, static_cast<size_t>(g.n));
+            gp::to_device(d, dmap.get(), map, static_cast<size_t>(g.n));
+            gp::Buf<W> cvw(d, static_cast<size_t>(coarse_n));
+            cvw.zero(d);
+            launch(d, "coarse_weights_kernel", gp::coarse_weights_kernel<W>, gp::blocks_for(g.n, gp::kThreads), gp::kThreads, 0, 
+                g.n, dmap.get(), g.vwp(), cvw.get());
+            GP_LAUNCH();
+            gp::DGraph<T> c;
+            gp::contract<T>(d, g, dmap.get(), coarse_n, std::move(cvw), c);
+            std::vector<int64_t> off;
+            std::vector<int32_t> nbr, mp;
+            std::vector<uint64_t> ew, vw;
+            gp::host_level_copy<T>(d, c, nullptr, 0, off, nbr, ew, vw, mp);
+            std::copy(off.begin(), off.end(), offsets);
+            std::copy(nbr.begin(), nbr.end(), neighbors);
+            std::copy(ew.begin(), ew.end(), edge_weights);
+            std::copy(vw.begin(), vw.end(), vertex_weights);
+            *coarse_m = c.m;
+        });
+    });
+}
+
+gp_status gp_coarsen(gp_ctx* ctx, const gp_graph* graph, const gp_options* options, gp_hierarchy** out) {
+    if (!ctx || !out) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        const gp::Opts o = gp::to_opts(options);
+        gp::Log log;
+        log.on = options && options->log;
+        auto res = std::make_unique<gp_hierarchy>();
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, o.verify);
+            gp::Hierarchy<T> h;
+            gp::coarsen<T>(d, std::move(g), o, h, log);
+            res->stop_reason = h.stop_reason;
+            for (size_t i = 0; i < h.levels.size(); ++i) {
+                gp_hierarchy::Level L;
+                const gp::i32* mp = i < h.maps.size() ? h.maps[i].get() : nullptr;
+                gp::host_level_copy<T>(d, h.levels[i], mp, h.levels[i].n, L.off, L.nbr, L.ew, L.vw, L.map);
+                res->levels.push_back(std::move(L));
+            }
+        });
+        *out = res.release();
+    });
+}
+
+int32_t gp_hierarchy_levels(const gp_hierarchy* h) { return h ? static_cast<int32_t>(h->levels.size()) : 0; }
+
+gp_status gp_hierarchy_level(const gp_hierarchy* h, int level, int64_t* n, int64_t* m, int64_t* offsets,
+                             int32_t* neighbors, uint64_t* edge_weights, uint64_t* vertex_weights,
+                             int32_t* map_to_next) {
+    if (!h || level < 0 || level >= static_cast<int>(h->levels.size())) return GP_EINVAL;
+    const auto& L = h->levels[level];
+    if (n) *n = static_cast<int64_t>(L.vw.size());
+    if (m) *m = static_cast<int64_t>(L.nbr.size());
+    if (offsets) std::copy(L.off.begin(), L.off.end(), offsets);
+    if (neighbors) std::copy(L.nbr.begin(), L.nbr.end(), neighbors);
+    if (edge_weights) std::copy(L.ew.begin(), L.ew.end(), edge_weights);
+    if (vertex_weights) std::copy(L.vw.begin(), L.vw.end(), vertex_weights);
+    if (map_to_next) std::copy(L.map.begin(), L.map.end(), map_to_next);
+    return GP_OK;
+}
+
+gp_status gp_hierarchy_write(const gp_hierarchy* h, const char* path) {
+    if (!h || !path) return GP_EINVAL;
+    return guarded(nullptr, [&] {
+        const std::string tmp = std::string(path) + ".tmp";
+        {
+            std::ofstream o(tmp, std::ios::binary | std::ios::trunc);
+            if (!o) gp::fail(GP_ERUNTIME, "cannot open hierarchy temporary file");
+            auto put = [&](int32_t v) { o.write(reinterpret_cast<const char*>(&v), 4); };
+            put(static_cast<int32_t>(h->levels.size()));
+            for (size_t i = 0; i < h->levels.size(); ++i) {
+                const auto& L = h->levels[i];
+                if (L.vw.size() > static_cast<size_t>(INT32_MAX) || L.nbr.size() > static_cast<size_t>(INT32_MAX))
+                    gp::fail(GP_ERUNTIME, "hierarchy export requires 32-bit dimensions");
+                put(static_cast<int32_t>(L.vw.size()));
+                put(static_cast<int32_t>(L.nbr.size()));
+                for (auto x : L.off) put(static_cast<int32_t>(x));
+                for (auto x : L.nbr) put(x);
+                for (auto x : L.ew) {
+                    if (x > static_cast<uint64_t>(INT32_MAX)) gp::fail(GP_ERUNTIME, "hierarchy edge weight exceeds int32");
+                    put(static_cast<int32_t>(x));
+                }
+                for (auto x : L.vw) {
+                    if (x > static_cast<uint64_t>(INT32_MAX)) gp::fail(GP_ERUNTIME, "hierarchy vertex weight exceeds int32");
+                    put(static_cast<int32_t>(x));
+                }
+                if (i > 0) for (auto x : h->levels[i - 1].map) put(x);
+            }
+            o.flush();
+            if (!o) gp::fail(GP_ERUNTIME, "failed while writing hierarchy");
+        }
+        if (std::rename(tmp.c_str(), path) != 0) gp::fail(GP_ERUNTIME, "cannot commit hierarchy output");
+    });
+}
+
+void gp_hierarchy_free(gp_hierarchy* h) { delete h; }
+
+gp_status gp_initial_partition(gp_ctx* ctx, const gp_graph* graph, int parts, double ratio, uint32_t seed,
+                               int32_t* labels) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            gp::Buf<gp::i32> lab;
+            gp::Log log;
+            gp::initial_partition<T>(d, g, parts, ratio, seed, lab, nullptr, log);
+            gp::to_host(d, labels, lab.get(), static_cast<size_t>(g.n));
+            d.sync();
+        });
+    });
+}
+
+gp_status gp_diffusion(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int group, uint32_t seed, int steps,
+                       float* x) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            const gp::i32 n = static_cast<gp::i32>(g.n);
+            std::vector<gp::i32> members;
+            for (gp::i32 v = 0; v < n; ++v) if (labels[v] == group) members.push_back(v);
+            if (members.empty()) gp::fail(GP_EINVAL, "empty diffusion group");
+            gp::Buf<gp::i32> dl(d, static_cast<size_t>(n)), order(d, static_cast<size_t>(n)), top(d, static_cast<size_t>(n));
+            gp::to_device(d, dl.get(), labels, static_cast<size_t>(n));
+            std::vector<gp::i32> ord(members);
+            std::vector<gp::i32> tp(static_cast<size_t>(n), -1);
+            for (size_t i = 0; i < members.size(); ++i) tp[i] = 0;
+            ord.resize(static_cast<size_t>(n), 0);
+            gp::to_device(d, order.get(), ord.data(), ord.size());
+            gp::to_device(d, top.get(), tp.data(), tp.size());
+            gp::InitTask task{0, static_cast<gp::i32>(members.size()), group, 2, 0, -1, -1};
+            gp::Buf<gp::InitTask> dt(d, 1);
+            gp::to_device(d, dt.get(), &task, 1);
+            gp::Buf<float> deg(d, n), xa(d, n), xb(d, n), xo(d, n);
+            gp::Buf<gp::Moments> contrib(d, n);
+            gp::Buf<gp::u64> key(d, n);
+            gp::Buf<gp::u32> bar(d, 2);
+            xo.zero(d);
+            gp::launch_diffusion<T>(d, g, 1, dt.get(), top.get(), n, order.get(), dl.get(), seed, steps, deg.get(),
+                                    xa.get(), xb.get(), contrib.get(), xo.get(), key.get(), bar.get());
+            d.check_errors();
+            gp::to_host(d, x, xo.get(), static_cast<size_t>(n));
+            d.sync();
+        });
+    });
+}
+
+gp_status gp_refine(gp_ctx* ctx, const gp_graph* graph, int32_t* labels, int parts, double ratio, int max_rounds,
+                    int deterministic, gp_refine_stats* stats) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        if (parts < 2 || parts > 32 || max_rounds < 0 || max_rounds > 64 || !std::isfinite(ratio) || ratio < 1.0 ||
+            !graph || graph->n <= 0)
+            gp::fail(GP_EINVAL, "invalid refinement options");
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            for (gp::i64 v = 0; v < g.n; ++v)
+                if (labels[v] < 0 || labels[v] >= parts) gp::fail(GP_EINVAL, "refinement partition has an invalid part id");
+            gp::Buf<gp::i32> lab(d, static_cast<size_t>(g.n));
+            gp::to_device(d, lab.get(), labels, static_cast<size_t>(g.n));
+            gp::Buf<gp::u64> pw(d, 32);
+            std::vector<gp::u64> host_pw;
+            gp::part_weights<T>(d, g, lab.get(), parts, pw.get(), host_pw);
+            gp::u64 total = 0;
+            for (auto x : host_pw) total += x;
+            const gp::u64 cap = gp::partition_capacity(total, parts, ratio);
+            if (*std::max_element(host_pw.begin(), host_pw.end()) > cap)
+                gp::fail(GP_EINVAL, "initial refinement partition is imbalanced");
+            gp::RefineWork w;
+            const bool narrow = gp::narrow_cache(g, d);
+            auto st = gp::refine_dispatch<T>(d, g, w, lab.get(), pw.get(), host_pw, parts, cap, max_rounds,
+                                             deterministic != 0, false, narrow);
+            gp::to_host(d, labels, lab.get(), static_cast<size_t>(g.n));
+            d.sync();
+            if (stats) *stats = st;
+        });
+    });
+}
+
+uint64_t gp_launch_count(const gp_ctx* ctx) { return ctx ? ctx->dev.launches : 0; }
+
+void* gp_ctx_stream(const gp_ctx* ctx) { return ctx ? static_cast<void*>(ctx->dev.stream) : nullptr; }
+
+gp_status gp_profile_enable(gp_ctx* ctx, int on) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        auto& d = ctx->dev;
+        d.prof_resolve();
+        d.prof_table.clear();
+        d.prof = on != 0;
+    });
+}
+
+gp_status gp_profile_dump(gp_ctx* ctx, char* buffer, uint64_t capacity) {
+    if (!ctx || !buffer || capacity == 0) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        auto& d = ctx->dev;
+        d.prof_resolve();
+        std::ostringstream os;
+        os << std::setprecision(12);
+        for (const auto& kv : d.prof_table)
+            os << kv.first << ' ' << kv.second.launches << ' ' << kv.second.ms << ' ' << kv.second.bytes << '\n';
+        const std::string s = os.str();
+        const size_t n = std::min<size_t>(s.size(), static_cast<size_t>(capacity) - 1);
+        std::memcpy(buffer, s.data(), n);
+        buffer[n] = 0;
+    });
+}
+
+gp_status gp_cut(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts, uint64_t* directed_cut,
+                 uint64_t* loads) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        if (parts < 1 || parts > 32) gp::fail(GP_EINVAL, "invalid parts");
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            for (gp::i64 v = 0; v < g.n; ++v)
+                if (labels[v] < 0 || labels[v] >= parts) gp::fail(GP_EINVAL, "invalid label");
+            gp::Buf<gp::i32> lab(d, static_cast<size_t>(std::max<gp::i64>(g.n, 1)));
+            gp::to_device(d, lab.get(), labels, static_cast<size_t>(g.n));
+            gp::Buf<gp::u64> s(d, 2);
+            const gp::u64 c = gp::directed_cut<T>(d, g, lab.get(), s.get());
+            if (directed_cut) *directed_cut = c;
+            if (loads) {
+                gp::Buf<gp::u64> pw(d, 32);
+                std::vector<gp::u64> host;
+                gp::part_weights<T>(d, g, lab.get(), parts, pw.get(), host);
+                std::copy(host.begin(), host.end(), loads);
+            }
+        });
+    });
+}
+
+}  // extern "C"

@@ -136,15 +136,15 @@ void exclusive_scan(Device& d, F f, T* out, i64 n, T* total_dev = nullptr) {
     }
     const i64 tiles = (n + kScanTile - 1) / kScanTile;
     if (tiles == 1) {
-        scan_tiles_kernel<T, F><<<1, kThreads, 0, d.stream>>>(f, n, out, nullptr, total_dev);
+        launch(d, "scan_tiles_kernel", scan_tiles_kernel<T, F>, 1, kThreads, 0, f, n, out, nullptr, total_dev);
         GP_LAUNCH();
         return;
     }
     Buf<T> sums(d, static_cast<size_t>(tiles));
-    scan_tile_sums_kernel<T, F><<<static_cast<int>(tiles), kThreads, 0, d.stream>>>(f, n, sums.get());
+    launch(d, "scan_tile_sums_kernel", scan_tile_sums_kernel<T, F>, static_cast<int>(tiles), kThreads, 0, f, n, sums.get());
     GP_LAUNCH();
     exclusive_scan<T>(d, ArrayInput<T>{sums.get()}, sums.get(), tiles, nullptr);
-    scan_tiles_kernel<T, F><<<static_cast<int>(tiles), kThreads, 0, d.stream>>>(f, n, out, sums.get(), total_dev);
+    launch(d, "scan_tiles_kernel", scan_tiles_kernel<T, F>, static_cast<int>(tiles), kThreads, 0, f, n, out, sums.get(), total_dev);
     GP_LAUNCH();
 }
 
@@ -288,10 +288,10 @@ void radix_sort(Device& d, K* keys, V* vals, K* keys_alt, V* vals_alt, i64 n, in
     V* dst_v = vals_alt;
     int passes = 0;
     for (int shift = begin_bit; shift < end_bit; shift += 8, ++passes) {
-        radix_hist_kernel<K><<<grid, kThreads, 0, d.stream>>>(src_k, n, shift, hist.get());
+        launch(d, "radix_hist_kernel", radix_hist_kernel<K>, grid, kThreads, 0, src_k, n, shift, hist.get());
         GP_LAUNCH();
         exclusive_scan<i64>(d, U32ToI64{hist.get()}, offs.get(), static_cast<i64>(kRadix) * grid);
-        radix_scatter_kernel<K, V><<<grid, kThreads, 0, d.stream>>>(src_k, src_v, dst_k, dst_v, n, shift,
+        launch(d, "radix_scatter_kernel", radix_scatter_kernel<K, V>, grid, kThreads, 0, src_k, src_v, dst_k, dst_v, n, shift,
                                                                     offs.get());
         GP_LAUNCH();
         std::swap(src_k, dst_k);

@@ -1,0 +1,397 @@
+// Incremental bucketed refinement (src/refine_incremental.cuh:7-361,
+// src/refine.cu:52-142).  B200 layout:
+//
+// * the dense n x k affinity cache is u32 when the graph's total directed
+//   edge weight fits 32 bits (halving the dominant HBM stream), else u64;
+// * LP proposals append proposers to a list; the priority filter, the fused
+//   cache+cut update and the commit then touch proposers/movers only;
+// * list-driven kernels use a fixed grid with grid-stride loops so the host
+//   never has to size a launch from a device count;
+// * the rebalance ranks vertices inside a (source, gain bucket, section)
+//   bucket either with atomics in arbitrary order (the reference's
+//   behaviour) or, in deterministic mode, by (gain per weight descending,
+//   vertex ascending) through a stable radix sort, which makes labels
+//   bit-reproducible.
+#pragma once
+
+#include "gp_prim.cuh"
+
+namespace gp {
+
+constexpr int kBalBuckets = 50, kBalSections = 16, kBalWidth = kBalBuckets * kBalSections;
+
+struct RefineCounters {
+    i64 proposers;
+    i64 movers;
+    long long delta;      // cut decrease of the last apply
+    u64 directed_cut;
+    u64 pad[4];
+};
+
+__device__ __forceinline__ void cache_add(u32* p, u64 v) { atomicAdd(p, static_cast<u32>(v)); }
+__device__ __forceinline__ void cache_add(u64* p, u64 v) { atomic_add_u64(p, v); }
+
+// Exact directed cut, warp per vertex, one atomic per block
+// (refine_cut_kernel, src/refine.cu:52-87).
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) cut_kernel(i64 n, const O* __restrict__ off, const i32* __restrict__ nbr,
+                                                       const W* __restrict__ ew, const i32* __restrict__ labels,
+                                                       u64* out) {
+    __shared__ u64 sh[kWarps + 1];
+    const int lane = threadIdx.x & 31;
+    u64 local = 0;
+    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
+    for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); v < n; v += warps_total) {
+        const i32 s = labels[v];
+        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32)
+            if (labels[nbr[e]] != s) local += static_cast<u64>(weight_at(ew, e));
+    }
+    local = block_sum(local, sh);
+    if (threadIdx.x == 0 && local) atomic_add_u64(out, local);
+}
+
+// incremental_build_affinity (src/refine_incremental.cuh:7-25)
+template <typename O, typename W, typename C>
+__global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* __restrict__ off,
+                                                               const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                               const i32* __restrict__ labels, int k, C* cache) {
+    __shared__ u64 rows[kWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
+    for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + warp; v < n; v += warps_total) {
+        rows[warp][lane] = 0;
+        __syncwarp();
+        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
+            const i32 u = nbr[e];
+            if (u != v) atomicAdd(reinterpret_cast<unsigned long long*>(&rows[warp][labels[u]]),
+                                  static_cast<unsigned long long>(weight_at(ew, e)));
+        }
+        __syncwarp();
+        if (lane < k) cache[v * k + lane] = static_cast<C>(rows[warp][lane]);
+        __syncwarp();
+    }
+}
+
+// incremental_lp_proposals (src/refine_incremental.cuh:27-46); proposers
+// are appended to `list`.
+template <typename C>
+__global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i32* __restrict__ labels, int k,
+                                    double filter, unsigned char* locks, i32* targets, i64* gains, i32* list,
+                                    RefineCounters* ctr) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    targets[v] = -1;
+    gains[v] = INT64_MIN;
+    if (locks[v]) { locks[v] = 0; return; }
+    const i32 s = labels[v];
+    const C* row = cache + v * k;
+    u64 best = 0;
+    int target = -1;
+    for (int p = 0; p < k; ++p) {
+        const u64 c = static_cast<u64>(row[p]);
+        if (p != s && c > best) { best = c; target = p; }
+    }
+    const u64 current = static_cast<u64>(row[s]);
+    if (target >= 0 && (best >= current || current - best < static_cast<u64>(filter * static_cast<double>(current)))) {
+        targets[v] = target;
+        gains[v] = best >= current ? static_cast<i64>(best - current) : -static_cast<i64>(current - best);
+        const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->proposers), 1ULL);
+        list[slot] = static_cast<i32>(v);
+    }
+}
+
+// incremental_priority_filter (src/refine_incremental.cuh:48-67), warp per
+// proposer; movers are appended to `movers` and flagged.
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) priority_filter_kernel(
+    const i32* __restrict__ list, const RefineCounters* ctr_in, const O* __restrict__ off,
+    const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
+    const i32* __restrict__ targets, const i64* __restrict__ gains, unsigned char* flags, i32* movers,
+    RefineCounters* ctr) {
+    const int lane = threadIdx.x & 31;
+    const i64 count = ctr_in->proposers;
+    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
+    for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
+        const i32 v = list[i];
+        const i32 s = labels[v], t = targets[v];
+        const i64 g = gains[v];
+        long long corr = 0;
+        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
+            const i32 u = nbr[e];
+            if (u == v) continue;
+            const i32 tu = targets[u];
+            if (tu < 0) continue;
+            const i64 gu = gains[u];
+            if (!(gu > g || (gu == g && u < v))) continue;
+            const i32 lu = labels[u];
+            const auto w = static_cast<long long>(weight_at(ew, e));
+            corr += w * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+        }
+        corr = warp_sum(corr);
+        if (lane == 0 && g + corr >= 0) {
+            flags[v] = 1;
+            const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
+            movers[slot] = v;
+        }
+    }
+}
+
+// incremental_update_cache_and_cut (src/refine_incremental.cuh:69-95)
+template <typename O, typename W, typename C>
+__global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
+    const i32* __restrict__ movers, const RefineCounters* ctr_in, const O* __restrict__ off,
+    const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
+    const i32* __restrict__ targets, const unsigned char* __restrict__ flags, int k, C* cache, RefineCounters* ctr) {
+    __shared__ long long sh[kWarps + 1];
+    const int lane = threadIdx.x & 31;
+    const i64 count = ctr_in->movers;
+    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
+    long long gain = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
+        const i32 v = movers[i];
+        const i32 s = labels[v], t = targets[v];
+        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
+            const i32 u = nbr[e];
+            if (u == v) continue;
+            const u64 w = static_cast<u64>(weight_at(ew, e));
+            cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
+            cache_add(&cache[static_cast<i64>(u) * k + t], w);
+            const bool fu = flags[u] != 0;
+            if (!fu || u > v) {
+                const i32 lu = labels[u];
+                const i32 nn = fu ? targets[u] : lu;
+                gain += static_cast<long long>(w) * ((s != lu) - (t != nn));
+            }
+        }
+    }
+    gain = block_sum(gain, sh);
+    if (threadIdx.x == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));
+}
+
+// incremental_commit (src/refine_incremental.cuh:97-109); also clears the
+// mover flag so that `flags` is all-zero outside an apply.
+template <typename W>
+__global__ void commit_kernel(const i32* __restrict__ movers, const RefineCounters* ctr_in,
+                              i32* labels, const i32* __restrict__ targets, const W* __restrict__ vw, u64* pw,
+                              unsigned char* locks, unsigned char* flags, int lp) {
+    const i64 count = ctr_in->movers;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i32 v = movers[i];
+        const i32 s = labels[v], t = targets[v];
+        const u64 w = static_cast<u64>(weight_at(vw, v));
+        atomic_add_u64(&pw[s], 0ULL - w);
+        atomic_add_u64(&pw[t], w);
+        labels[v] = t;
+        if (lp) locks[v] = 1;
+        flags[v] = 0;
+    }
+}
+
+// Rebalance gain bucket (refine_incremental.cuh:167-171) restated with host
+// thresholds 1.5^j: for g < 0, 25 + the smallest j with -g <= 1.5^j,
+// clamped to [2, 49].
+struct BucketThresholds { double t[48]; };   // j = -23 .. 24
+
+__device__ __forceinline__ int gain_bucket(double g, const BucketThresholds& th) {
+    if (g > 0) return 0;
+    if (g == 0) return 1;
+    const double a = -g;
+    if (a <= th.t[0]) return 2;
+    int lo = 1, hi = 47;   // smallest index in [1,47] with a <= t[idx], else 48
+    if (a > th.t[47]) return 49;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a <= th.t[mid]) hi = mid; else lo = mid + 1;
+    }
+    return 25 + (lo - 23);
+}
+
+// incremental_rebalance_proposals + balance_source_histogram
+// (src/refine_incremental.cuh:111-186).  Atomic mode ranks here; the
+// deterministic mode appends candidates (ascending vertex order is restored by
+// the scan-based compaction that follows).
+template <typename C, typename W>
+__global__ void rebalance_proposals_kernel(i64 n, const C* __restrict__ cache, const i32* __restrict__ labels,
+                                           const W* __restrict__ vw, int k, const u64* __restrict__ pw, u64 cap,
+                                           BucketThresholds th, int deterministic, i32* targets, double* gpw,
+                                           i32* bucket, u64* rank, u64* counts) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    targets[v] = -1;
+    bucket[v] = -1;
+    const i32 s = labels[v];
+    if (pw[s] <= cap) return;
+    const u64 w = static_cast<u64>(weight_at(vw, v));
+    const C* row = cache + v * k;
+    int best = -1;
+    u64 best_conn = 0, best_slack = 0;
+    for (int p = 0; p < k; ++p) {
+        const u64 pp = pw[p];
+        if (p == s || pp >= cap || w > cap - pp) continue;
+        const u64 value = static_cast<u64>(row[p]);
+        const u64 slack = cap - pp;
+        if (best < 0 || value > best_conn || (value == best_conn && slack > best_slack)) {
+            best = p; best_conn = value; best_slack = slack;
+        }
+    }
+    if (best >= 0 && best_conn == 0) {
+        u64 total_slack = 0;
+        for (int p = 0; p < k; ++p) {
+            const u64 pp = pw[p];
+            if (p != s && pp < cap && w <= cap - pp)
+                total_slack = UINT64_MAX - total_slack < cap - pp ? UINT64_MAX : total_slack + cap - pp;
+        }
+        u64 ticket = static_cast<u64>(mix32(static_cast<u32>(v))) % total_slack;
+        for (int p = 0; p < k; ++p) {
+            const u64 pp = pw[p];
+            if (p == s || pp >= cap || w > cap - pp) continue;
+            const u64 slack = cap - pp;
+            if (ticket < slack) { best = p; break; }
+            ticket -= slack;
+        }
+    }
+    if (best < 0) return;
+    const u64 current = static_cast<u64>(row[s]);
+    const double gain = best_conn >= current ? static_cast<double>(best_conn - current)
+                                             : -static_cast<double>(current - best_conn);
+    const double g = gain / static_cast<double>(w);
+    targets[v] = best;
+    gpw[v] = g;
+    const int b = s * kBalWidth + gain_bucket(g, th) * kBalSections + static_cast<int>(mix32(static_cast<u32>(v)) % kBalSections);
+    bucket[v] = b;
+    if (!deterministic) rank[v] = atomic_add_u64(&counts[b], w);
+}
+
+// balance_scan_buckets (src/refine_incremental.cuh:188-202): exclusive scan
+// of the 800 buckets of each part, block per part.
+__global__ void __launch_bounds__(kThreads) bucket_scan_kernel(const u64* counts, u64* offsets) {
+    __shared__ u64 sh[kWarps + 1];
+    constexpr int kPer = (kBalWidth + kThreads - 1) / kThreads;   // 4
+    u64 vals[kPer];
+    u64 local = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int b = threadIdx.x * kPer + i;
+        vals[i] = b < kBalWidth ? counts[blockIdx.x * kBalWidth + b] : 0;
+        local += vals[i];
+    }
+    u64 run = block_exclusive_sum(local, sh, static_cast<u64*>(nullptr));
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int b = threadIdx.x * kPer + i;
+        if (b < kBalWidth) offsets[blockIdx.x * kBalWidth + b] = run;
+        run += vals[i];
+    }
+}
+
+// balance_select_sources (src/refine_incremental.cuh:204-217)
+template <typename W>
+__global__ void select_sources_kernel(i64 n, i32* bucket, u64* rank, const u64* offsets, const u64* pw, u64 cap,
+                                      const i32* targets, const W* vw, int deterministic, u64* counts) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n || bucket[v] < 0) return;
+    const int b = bucket[v], s = b / kBalWidth;
+    if (offsets[b] + rank[v] >= pw[s] - cap) { bucket[v] = -1; return; }
+    const int d = targets[v] * kBalWidth + b % kBalWidth;
+    bucket[v] = d;
+    if (!deterministic) rank[v] = atomic_add_u64(&counts[d], static_cast<u64>(weight_at(vw, v)));
+}
+
+// balance_select_destinations (src/refine_incremental.cuh:219-232)
+template <typename W>
+__global__ void select_destinations_kernel(i64 n, const i32* bucket, const u64* rank, const u64* offsets,
+                                           const u64* pw, u64 cap, const W* vw, unsigned char* flags, i32* movers,
+                                           RefineCounters* ctr) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int b = bucket[v];
+    if (b < 0) return;
+    const u64 before = offsets[b] + rank[v];
+    const u64 slack = cap - pw[b / kBalWidth];
+    if (before <= slack && static_cast<u64>(weight_at(vw, v)) <= slack - before) {
+        flags[v] = 1;
+        const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
+        movers[slot] = static_cast<i32>(v);
+    }
+}
+
+// Deterministic ranks: candidates (bucket >= 0) compacted in vertex order,
+// sorted by (bucket asc, gain per weight desc); rank = weight prefix inside
+// the bucket; counts = bucket totals.
+struct HasBucket {
+    const i32* bucket;
+    __device__ i64 operator()(i64 i) const { return bucket[i] >= 0 ? 1 : 0; }
+};
+
+__global__ void compact_bucket_kernel(i64 n, const i32* bucket, const i64* pos, i32* list) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n && bucket[v] >= 0) list[pos[v]] = static_cast<i32>(v);
+}
+
+// mode 0: ~orderable(gpw) (desc); mode 1: bucket
+__global__ void rank_keys_kernel(i64 count, const i32* list, const double* gpw, const i32* bucket, int mode, u64* keys) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const i32 v = list[i];
+    if (mode == 0) {
+        double g = gpw[v];
+        if (g == 0.0) g = 0.0;
+        const u64 b = static_cast<u64>(__double_as_longlong(g));
+        const u64 ord = (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
+        keys[i] = ~ord;
+    } else {
+        keys[i] = static_cast<u64>(bucket[v]);
+    }
+}
+
+template <typename W>
+struct ListWeight {
+    const i32* list;
+    const W* vw;
+    __device__ u64 operator()(i64 i) const { return static_cast<u64>(weight_at(vw, list[i])); }
+};
+
+__global__ void bucket_heads_kernel(i64 count, const i32* list, const i32* bucket, const u64* excl, u64* bucket_base) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int b = bucket[list[i]];
+    if (i == 0 || bucket[list[i - 1]] != b) bucket_base[b] = excl[i];
+}
+
+template <typename W>
+__global__ void bucket_ranks_kernel(i64 count, const i32* list, const i32* bucket, const u64* excl,
+                                    const u64* bucket_base, const W* vw, u64* rank, u64* counts) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const i32 v = list[i];
+    const int b = bucket[v];
+    rank[v] = excl[i] - bucket_base[b];
+    if (i + 1 == count || bucket[list[i + 1]] != b)
+        counts[b] = excl[i] + static_cast<u64>(weight_at(vw, v)) - bucket_base[b];
+}
+
+__global__ void project_kernel(i64 n, const i32* map, const i32* coarse, i32* fine) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v < n) fine[v] = coarse[map[v]];
+}
+
+template <typename W>
+__global__ void max_weight_kernel(i64 m, const W* ew, u64* out) {
+    u64 mx = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        mx = static_cast<u64>(ew[i]) > mx ? static_cast<u64>(ew[i]) : mx;
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomic_max_u64(out, mx);
+}
+
+template <typename W>
+__global__ void sum_weight_kernel(i64 m, const W* ew, u64* out) {
+    __shared__ u64 sh[kWarps + 1];
+    u64 s = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x)
+        s += static_cast<u64>(ew[i]);
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0 && s) atomic_add_u64(out, s);
+}
+
+}  // namespace gp

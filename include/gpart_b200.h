@@ -44,11 +44,13 @@ enum { GP_MEMORY_HOST = 0, GP_MEMORY_DEVICE = 1 };
 
 /* A symmetric CSR graph.  With index64 = 0 the arrays use the width's types:
  * offsets int32 (standard) / int64 (big), neighbours int32, weights
- * uint32 / uint64.  With index64 = 1 offsets and neighbours are the int64
- * arrays of the reference's input files (src/graph.cpp:47-122); the library
- * narrows and validates them on the GPU with the reference's rules and
- * messages.  NULL weights mean unit weights (the reference's file input always
- * has unit weights, src/graph.cpp:117-118). */
+ * uint32 / uint64; device arrays in these types are used in place, without a
+ * copy, and must stay valid and unmodified during the call.  With index64 = 1
+ * offsets and neighbours are the int64 arrays of the reference's input files
+ * (src/graph.cpp:47-122); the library narrows and validates them on the GPU
+ * with the reference's rules and messages.  NULL weights mean unit weights
+ * (the reference's file input always has unit weights,
+ * src/graph.cpp:117-118). */
 typedef struct gp_graph {
     int64_t n;
     int64_t m;
@@ -174,6 +176,22 @@ gp_status gp_refine(gp_ctx* ctx, const gp_graph* graph, int32_t* labels, int par
  * tools/verify_partition.py:22-65 and src/graph.cpp:192-212). */
 gp_status gp_cut(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts,
                  uint64_t* directed_cut, uint64_t* loads);
+
+/* Kernel launches issued by this context so far (all of them are the
+ * library's own sm_100a kernels). */
+uint64_t gp_launch_count(const gp_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events with the library's. */
+void* gp_ctx_stream(const gp_ctx* ctx);
+
+/* Per-kernel CUDA-event timing on the context stream (off by default).
+ * Enabling (or disabling) clears the table. */
+gp_status gp_profile_enable(gp_ctx* ctx, int on);
+/* Writes one line per kernel: "<name> <launches> <milliseconds> <algorithmic
+ * bytes>" (bytes are recorded for the kernels whose traffic model is known,
+ * else 0). */
+gp_status gp_profile_dump(gp_ctx* ctx, char* buffer, uint64_t capacity);
 
 #ifdef __cplusplus
 }
