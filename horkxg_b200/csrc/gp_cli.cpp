@@ -37,12 +37,25 @@
 
 namespace {
 
+// Page-locked staging for the input arrays (fast H2D); plain host memory
+// when page-locking is unavailable.
 struct Pinned {
     void* p = nullptr;
+    bool pinned = false;
     explicit Pinned(size_t bytes) {
-        if (bytes && cudaMallocHost(&p, bytes) != cudaSuccess) throw std::runtime_error("cannot allocate pinned host memory");
+        if (!bytes) return;
+        if (cudaMallocHost(&p, bytes) == cudaSuccess) {
+            pinned = true;
+        } else {
+            cudaGetLastError();
+            p = std::malloc(bytes);
+            if (!p) throw std::runtime_error("cannot allocate host memory");
+        }
     }
-    ~Pinned() { if (p) cudaFreeHost(p); }
+    ~Pinned() {
+        if (!p) return;
+        if (pinned) cudaFreeHost(p); else std::free(p);
+    }
     int64_t* i64() const { return static_cast<int64_t*>(p); }
 };
 

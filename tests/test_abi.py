@@ -1,0 +1,113 @@
+"""CPU tests of the product boundary: the C-ABI library loads and exports
+every symbol include/gpart_b200.h declares; host-only entry points; the
+drop-in drivers' argument and input errors (they fail before any CUDA call);
+generator determinism."""
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import horkxg_b200 as hb
+from horkxg_b200 import graphs
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "gpart_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(gp_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_symbols()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", str(hb.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT (gp_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    lib = hb.lib()
+    for n in names:
+        getattr(lib, n)
+    assert set(hb.EXPORTS) <= set(names)
+
+
+def test_library_is_sm100a():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(hb.LIB_PATH)], capture_output=True,
+                         text=True).stdout
+    assert "sm_100a" in out
+
+
+@pytest.mark.parametrize("total,parts,ratio,expected", [(6, 2, 1.10, 3), (100, 4, 1.03, 25), (1000, 4, 1.03, 257),
+                                                        (6, 2, 1.34, 4)])
+def test_host_capacity(total, parts, ratio, expected):
+    assert hb.capacity(total, parts, ratio) == expected
+
+
+@pytest.mark.parametrize("total,parts,ratio,status", [(4, 3, 1.03, hb.GP_EINVAL), (100, 0, 1.03, hb.GP_EINVAL),
+                                                      (100, 33, 1.03, hb.GP_EINVAL), (100, 4, 0.99, hb.GP_EINVAL),
+                                                      (100, 4, float("nan"), hb.GP_EINVAL),
+                                                      (2**64 - 1, 2, 4.0, hb.GP_EOVERFLOW)])
+def test_host_capacity_rejections(total, parts, ratio, status):
+    with pytest.raises(hb.PartitionError) as e:
+        hb.capacity(total, parts, ratio)
+    assert e.value.status == status
+
+
+def driver(width="standard"):
+    return str(hb.BIN / f"gpart_partition_{width}")
+
+
+@pytest.mark.parametrize("width", ["standard", "big"])
+def test_driver_usage_exit_code(width):
+    r = subprocess.run([driver(width), "a", "b"], capture_output=True, text=True)
+    assert r.returncode == 2 and "Usage:" in r.stderr
+
+
+def test_driver_missing_file(tmp_path):
+    r = subprocess.run([driver(), str(tmp_path / "no"), str(tmp_path / "no2"), "4", str(tmp_path / "o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and r.stderr.startswith("gpart_partition: cannot open")
+
+
+def test_driver_bad_sizes(tmp_path):
+    (tmp_path / "p").write_bytes(b"\0" * 12)
+    (tmp_path / "i").write_bytes(b"")
+    r = subprocess.run([driver(), str(tmp_path / "p"), str(tmp_path / "i"), "2", str(tmp_path / "o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "invalid binary size" in r.stderr
+    np.array([0, 1, 1], np.int64).tofile(tmp_path / "p")
+    np.array([0, 0], np.int64).tofile(tmp_path / "i")
+    r = subprocess.run([driver(), str(tmp_path / "p"), str(tmp_path / "i"), "2", str(tmp_path / "o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "CSR offsets do not match indices" in r.stderr
+
+
+def test_driver_infeasible_capacity(tmp_path):
+    np.array([0, 0, 0, 0, 0], np.int64).tofile(tmp_path / "p")
+    np.array([], np.int64).tofile(tmp_path / "i")
+    r = subprocess.run([driver(), str(tmp_path / "p"), str(tmp_path / "i"), "3", str(tmp_path / "o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "capacity" in r.stderr
+
+
+def test_generators_deterministic(tmp_path, monkeypatch):
+    monkeypatch.setenv("GP_GRAPH_CACHE", str(tmp_path / "a"))
+    a = [p.read_bytes() for p in graphs.rmat(10)]
+    monkeypatch.setenv("GP_GRAPH_CACHE", str(tmp_path / "b"))
+    b = [p.read_bytes() for p in graphs.rmat(10)]
+    assert a == b
+    off, idx = np.frombuffer(a[0], np.int64), np.frombuffer(a[1], np.int64)
+    src = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    assert (src != idx).all()
+    key = np.sort(src * (len(off) - 1) + idx)
+    assert np.array_equal(key, np.sort(idx * (len(off) - 1) + src))
+    assert (np.diff(key) > 0).all()
+
+
+def test_grid_sizes():
+    off, idx = graphs.load(*graphs.grid2d(256, 256))
+    assert len(off) - 1 == 65536 and len(idx) == 261120

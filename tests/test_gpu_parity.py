@@ -1,0 +1,306 @@
+"""GPU parity tests: the sm_100a library, called through its C ABI, against the
+reference's golden vectors and the CPU oracle (bit-exact for every integer
+stage; FP32 diffusion within 1e-5 relative L2 of the FP64 oracle)."""
+import hashlib
+import re
+import statistics
+import subprocess
+
+import numpy as np
+import pytest
+
+import horkxg_b200 as hb
+import pyoracle as O
+from horkxg_b200 import graphs
+from helpers import goldens, csr_from_rows, weighted_stress
+from test_oracle import EXCHANGE, REPAIR, contraction_fixture, hub_path_259
+
+pytestmark = pytest.mark.gpu
+GOLD = goldens()
+WIDTH = {"standard": hb.STANDARD, "big": hb.BIG}
+DIFFUSION_TOL = 1e-5   # relative L2, FP32 device vs FP64 oracle
+
+
+def file_graph(name, width="standard"):
+    off, idx = graphs.load(*graphs.by_name(name))
+    return off, np.asarray(idx), hb.HostGraph(off, idx, width=WIDTH[width], index64=True)
+
+
+def digests(levels):
+    out = []
+    for i, (off, nbr, ew, vw, _) in enumerate(levels):
+        parts = [np.array([len(vw), len(nbr)], np.int32), off.astype(np.int32), nbr.astype(np.int32),
+                 ew.astype(np.int32), vw.astype(np.int32)]
+        if i > 0:
+            parts.append(levels[i - 1][4].astype(np.int32))
+        out.append({"n": len(vw), "m": len(nbr), "sha256": hashlib.sha256(b"".join(p.tobytes() for p in parts)).hexdigest()})
+    return out
+
+
+# --- SCLP hierarchy against the reference build (bit-exact, per level)
+@pytest.mark.parametrize("case", GOLD["hierarchies"],
+                         ids=lambda h: f"{h['fixture']}-k{h['parts']}-s{h['seed']}-{h['variant']}")
+def test_hierarchy_matches_reference(ctx, case):
+    _, _, g = file_graph(case["fixture"], case["variant"])
+    levels = ctx.coarsen(g, parts=case["parts"], seed=case["seed"], cluster_size_factor=case["beta"],
+                         pack_isolated=case["pack_isolated"])
+    assert digests(levels) == case["levels"]
+
+
+# --- aggregation against the oracle on weighted inputs (duplicates, self
+# loops, every degree class incl. global-hash hubs)
+@pytest.mark.parametrize("width", ["standard", "big"])
+@pytest.mark.parametrize("k", [2, 8, 32])
+def test_aggregate_weighted_stress(ctx, width, k):
+    off, nbr, ew, vw, _ = weighted_stress(k=4, scale=1 if width == "standard" else 1 << 35)
+    g = hb.HostGraph(off, nbr, ew, vw, width=WIDTH[width], index64=True)
+    for level, pack in ((0, False), (3, True)):
+        mp, cn, cap = ctx.aggregate(g, k, 11, level, 2, pack)
+        omp, ocn, ocap = O.aggregate(O.Graph(off, nbr, ew, vw), k, 11, level, 2, pack)
+        assert (cn, cap) == (ocn, ocap) and np.array_equal(mp, omp)
+
+
+@pytest.mark.parametrize("weight", [1, 1000000])
+def test_aggregate_cycle_hub_weights(ctx, weight):
+    off, idx, _ = file_graph("cycle_hub_4096")
+    ew = np.full(len(idx), weight, np.uint64)
+    g = hb.HostGraph(off, idx, ew, width=hb.STANDARD, index64=True)
+    for level in range(3):
+        mp, cn, cap = ctx.aggregate(g, 4, level, level, 256, False)
+        omp, ocn, ocap = O.aggregate(O.Graph(off, idx, ew), 4, level, level, 256, False)
+        assert (cn, cap) == (ocn, ocap) and np.array_equal(mp, omp)
+
+
+@pytest.mark.parametrize("name,k", [("rmat16", 32), ("rgg_20k", 8), ("grid3d_24", 4)])
+def test_aggregate_random_weights(ctx, name, k):
+    off, idx, _ = file_graph(name)
+    rng = np.random.default_rng(5)
+    # symmetric random edge weights: w(u,v) = h(min,max)
+    src = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    a, b = np.minimum(src, idx), np.maximum(src, idx)
+    ew = ((a * 2654435761 + b * 40503) % 97 + 1).astype(np.uint64)
+    vw = rng.integers(1, 4, len(off) - 1).astype(np.uint64)
+    g = hb.HostGraph(off, idx, ew, vw, width=hb.STANDARD, index64=True)
+    mp, cn, cap = ctx.aggregate(g, k, 3, 1, 64, True)
+    omp, ocn, ocap = O.aggregate(O.Graph(off, idx, ew, vw), k, 3, 1, 64, True)
+    assert (cn, cap) == (ocn, ocap) and np.array_equal(mp, omp)
+
+
+# --- contraction (tests/test_uncoarsen.cu:163-231)
+@pytest.mark.parametrize("width", ["standard", "big"])
+@pytest.mark.parametrize("groups", [7, 1, 7])
+def test_contraction_fixture(ctx, width, groups):
+    weight = 3 if width == "standard" else 1 << 40
+    off, nbr, ew, mapping, expected = contraction_fixture(groups, weight=weight)
+    g = hb.HostGraph(off, nbr, ew, width=WIDTH[width], index64=True)
+    coff, cnbr, cew, cvw = ctx.contract(g, mapping, groups)
+    o = O.contract(O.Graph(off, nbr, ew), mapping, groups)
+    assert list(coff) == list(o.off) and list(cnbr) == list(o.nbr) and list(cew) == list(o.ew)
+    assert list(cvw) == list(o.vw)
+
+
+def test_identity_and_empty_contraction(ctx):
+    off = np.array([0, 1, 3, 5, 6]); nbr = np.array([1, 0, 2, 1, 3, 2]); ew = np.array([1, 1, 5, 5, 10, 10])
+    coff, cnbr, cew, _ = ctx.contract(hb.HostGraph(off, nbr, ew, index64=True), np.arange(4), 4)
+    assert list(coff) == list(off) and list(cnbr) == list(nbr) and list(cew) == list(ew)
+    coff, cnbr, cew, _ = ctx.contract(hb.HostGraph(np.zeros(5, np.int64), np.zeros(0, np.int64), index64=True),
+                                      np.arange(4), 4)
+    assert list(coff) == [0] * 5 and len(cnbr) == 0
+
+
+@pytest.mark.parametrize("name,groups", [("rmat14", 700), ("rmat16", 40), ("grid2d_256", 9000)])
+def test_contraction_random_maps(ctx, name, groups):
+    off, idx, g = file_graph(name)
+    rng = np.random.default_rng(groups)
+    mapping = rng.integers(0, groups, len(off) - 1).astype(np.int32)
+    mapping[:groups] = np.arange(groups)   # every coarse id used
+    coff, cnbr, cew, cvw = ctx.contract(g, mapping, groups)
+    o = O.contract(O.Graph(off, idx), mapping, groups)
+    assert np.array_equal(coff, o.off) and np.array_equal(cnbr, o.nbr) and np.array_equal(cew, o.ew)
+
+
+# --- FP32 diffusion vs FP64 oracle (src/initial_partition_gpu.cu:81-142)
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("name", ["grid2d_64", "rmat12", "rgg_20k", "cycle_hub_4096"])
+def test_diffusion_root_task(ctx, name):
+    off, idx, g = file_graph(name)
+    labels = np.zeros(len(off) - 1, np.int32)
+    x = ctx.diffusion(g, labels, 0, 0, 64).astype(np.float64)
+    ref = O.diffusion(O.Graph(off, idx), labels, 0, 0, 64)
+    assert rel_l2(x, ref) < DIFFUSION_TOL
+
+
+def test_diffusion_subgroup_and_coarse_level(ctx):
+    # a second-depth task (group 16 of a split) on a contracted level
+    off, idx, g = file_graph("rmat14")
+    levels = ctx.coarsen(g, parts=32)
+    coff, cnbr, cew, cvw, _ = levels[-1]
+    n = len(cvw)
+    labels = np.where(np.arange(n) % 3 == 0, 16, 0).astype(np.int32)
+    cg = hb.HostGraph(coff, cnbr, cew, cvw, width=hb.STANDARD, index64=False)
+    for group, seed in ((16, 7), (0, 123)):
+        x = ctx.diffusion(cg, labels, group, seed, 64).astype(np.float64)
+        ref = O.diffusion(O.Graph(coff, cnbr, cew, cvw), labels, group, seed, 64)
+        assert rel_l2(x, ref) < DIFFUSION_TOL
+
+
+# --- initial partition (tests/test_initial_partition_gpu.cu:13-100)
+def test_initial_partition_fixtures(ctx):
+    rows = [[u for u in range(8) if u != v and u // 4 == v // 4] for v in range(8)]
+    off, nbr, _ = csr_from_rows(rows)
+    g = hb.HostGraph(off, nbr, np.full(len(nbr), 3), np.full(8, 2), index64=True)
+    a, b = ctx.initial_partition(g, 2), ctx.initial_partition(g, 2)
+    assert np.array_equal(a, b) and ctx.cut(g, a, 2)[0] == 0
+    gb = hb.HostGraph(off, nbr, np.full(len(nbr), 1 << 40), np.full(8, 1 << 40), width=hb.BIG, index64=True)
+    assert ctx.cut(gb, ctx.initial_partition(gb, 2), 2)[0] == 0
+    iso = hb.HostGraph(np.zeros(13, np.int64), np.zeros(0, np.int64), index64=True)
+    lab = ctx.initial_partition(iso, 3)
+    assert np.bincount(lab, minlength=3).max() <= hb.capacity(12, 3, 1.03)
+    hp = hub_path_259()
+    ghp = hb.HostGraph(hp.off, hp.nbr, hp.ew, index64=True)
+    for k in (2, 3, 4, 8):
+        lab = ctx.initial_partition(ghp, k)
+        assert np.array_equal(lab, ctx.initial_partition(ghp, k))
+        assert np.bincount(lab, minlength=k).max() <= hb.capacity(259, k, 1.03)
+    lab = ctx.initial_partition(hb.HostGraph(np.zeros(257, np.int64), np.zeros(0, np.int64), index64=True), 32)
+    assert np.bincount(lab, minlength=32).max() <= hb.capacity(256, 32, 1.03)
+
+
+def test_initial_partition_rejections(ctx):
+    heavy = np.ones(256, np.uint64); heavy[0] = 1000
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.initial_partition(hb.HostGraph(np.zeros(257, np.int64), np.zeros(0, np.int64), None, heavy,
+                                           index64=True), 3, 1.10)
+    assert e.value.status == hb.GP_EINVAL
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.initial_partition(hb.HostGraph(np.zeros(5, np.int64), np.zeros(0, np.int64), index64=True), 3)
+    assert e.value.status == hb.GP_EINVAL
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.initial_partition(hb.HostGraph(np.zeros(4, np.int64), np.zeros(0, np.int64), None, np.full(3, 2),
+                                           index64=True), 2)
+    assert e.value.status == hb.GP_ERUNTIME
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.initial_partition(hb.HostGraph([0, 1, 2], [1, 0], np.full(2, 2**64 - 1, np.uint64), width=hb.BIG,
+                                           index64=True), 2)
+    assert e.value.status == hb.GP_EOVERFLOW
+
+
+# --- refinement: deterministic mode is bit-exact with the oracle
+def refine_both(ctx, off, nbr, ew, vw, labels, k, width=hb.STANDARD):
+    g = hb.HostGraph(off, nbr, ew, vw, width=width, index64=True)
+    lab, st = ctx.refine(g, labels, k, 1.03, 32, True)
+    olab, ost = O.refine(O.Graph(off, nbr, ew, vw), labels, k, 1.03, 32)
+    return g, lab, st, olab, ost
+
+
+def test_refine_exchange_and_repair(ctx):
+    g, lab, st, olab, ost = refine_both(ctx, EXCHANGE["off"], EXCHANGE["nbr"], EXCHANGE["ew"], None,
+                                        EXCHANGE["labels"], 2)
+    assert np.array_equal(lab, olab) and ctx.cut(g, lab, 2)[0] // 2 == 2 and (lab == 0).sum() == 3
+    g, lab, st, olab, ost = refine_both(ctx, REPAIR["off"], REPAIR["nbr"], REPAIR["ew"], None, REPAIR["labels"], 2)
+    assert np.array_equal(lab, olab) and ctx.cut(g, lab, 2)[0] // 2 == 1 and (lab == 0).sum() == 4
+    assert st.admission_iterations > 0 and st.admission_iterations == ost.admission_iterations
+
+
+@pytest.mark.parametrize("width", ["standard", "big"])
+@pytest.mark.parametrize("k", [2, 4, 8, 32])
+def test_refine_weighted_stress_bit_exact(ctx, width, k):
+    off, nbr, ew, vw, labels = weighted_stress(k=k, scale=1 if width == "standard" else 1 << 35)
+    g, lab, st, olab, ost = refine_both(ctx, off, nbr, ew, vw, labels, k, WIDTH[width])
+    assert np.array_equal(lab, olab)
+    assert (st.rounds, st.initial_cut, st.final_cut) == (ost.rounds, ost.initial_cut, ost.final_cut)
+    loads = np.bincount(lab, weights=vw.astype(float), minlength=k)
+    assert loads.max() <= hb.capacity(int(vw.sum()), k, 1.03) and st.final_cut <= st.initial_cut
+
+
+@pytest.mark.parametrize("name,k", [("rmat12", 8), ("grid2d_64", 4), ("rgg_20k", 16)])
+def test_refine_projected_partition_bit_exact(ctx, name, k):
+    off, idx, _ = file_graph(name)
+    n = len(off) - 1
+    labels = (np.arange(n) * k // n).astype(np.int32)   # balanced blocks by id
+    g, lab, st, olab, ost = refine_both(ctx, off, idx, None, None, labels, k)
+    assert np.array_equal(lab, olab) and st.final_cut == ost.final_cut
+
+
+# --- full pipeline
+@pytest.mark.parametrize("fixture,k", sorted({(p["fixture"], p["parts"]) for p in GOLD["partitions"]}))
+def test_partition_recount_capacity_and_quality(ctx, fixture, k):
+    off, idx, g = file_graph(fixture)
+    cuts = []
+    for seed in range(5):
+        labels, rep = ctx.partition(g, parts=k, seed=seed)
+        cut, loads = O.recount(O.Graph(off, idx), labels, k)
+        assert cut // 2 == rep.cut                        # exact recount
+        assert loads.max() <= hb.capacity(len(off) - 1, k, 1.03)   # zero capacity violations
+        assert list(loads) == list(rep.part_weights)[:k]
+        cuts.append(rep.cut)
+    ref = statistics.median(p["cut"] for p in GOLD["partitions"] if p["fixture"] == fixture and p["parts"] == k)
+    assert statistics.median(cuts) <= 1.01 * ref, (cuts, ref)
+
+
+def test_deterministic_mode_is_bit_reproducible(ctx):
+    _, _, g = file_graph("rmat14")
+    a, ra = ctx.partition(g, parts=32, deterministic=1)
+    b, rb = ctx.partition(g, parts=32, deterministic=1)
+    assert np.array_equal(a, b) and ra.cut == rb.cut
+
+
+def test_partition_big_width_matches_standard_hierarchy(ctx):
+    _, _, gs = file_graph("grid3d_24", "standard")
+    _, _, gb = file_graph("grid3d_24", "big")
+    ls = ctx.coarsen(gs, parts=8)
+    lb = ctx.coarsen(gb, parts=8)
+    assert digests(ls) == digests(lb)
+    a, _ = ctx.partition(gs, parts=8, deterministic=1)
+    b, _ = ctx.partition(gb, parts=8, deterministic=1)
+    assert np.array_equal(a, b)
+
+
+def test_invalid_input_errors(ctx):
+    # 8 vertices, k=2: capacity 4 is feasible, so the CSR checks decide
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.partition(hb.HostGraph([0, 2, 1, 2, 2, 2, 2, 2, 2], [1, 2], index64=True), parts=2)
+    assert e.value.status == hb.GP_ERUNTIME and "monotone" in str(e.value)
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.partition(hb.HostGraph([0, 1, 2, 2, 2, 2, 2, 2, 2], [1, 9], index64=True), parts=2)
+    assert e.value.status == hb.GP_ERUNTIME and "out of range" in str(e.value)
+    with pytest.raises(hb.PartitionError) as e:
+        ctx.partition(hb.HostGraph([0, 0, 0], [], index64=True), parts=2)
+    assert e.value.status == hb.GP_EINVAL
+
+
+def test_driver_end_to_end(tmp_path):
+    indptr, indices = graphs.by_name("grid2d_256")
+    out = tmp_path / "labels.bin"
+    r = subprocess.run([str(hb.BIN / "gpart_partition_standard"), str(indptr), str(indices), "4", str(out),
+                        "1.03", "0"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    cut = int(re.findall(r"^final_edge_cut=(\d+)$", r.stdout, re.M)[-1])
+    timing = re.findall(r"partition_timing (.*)", r.stdout)[-1]
+    for key in ("algorithm_total_seconds", "wall_total_seconds", "coarsen_seconds", "input_prepare_seconds"):
+        assert f"{key}=" in timing
+    labels = np.fromfile(out, np.int32)
+    off, idx = graphs.load(indptr, indices)
+    rc, loads = O.recount(O.Graph(off, np.asarray(idx)), labels, 4)
+    assert rc // 2 == cut and loads.max() <= hb.capacity(65536, 4, 1.03)
+
+
+def test_coarsen_driver_writes_reference_format(tmp_path):
+    indptr, indices = graphs.by_name("cycle_hub_4096")
+    out = tmp_path / "h.bin"
+    r = subprocess.run([str(hb.BIN / "gpart_coarsen_standard"), str(indptr), str(indices), "4", str(out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    case = next(h for h in GOLD["hierarchies"] if h["fixture"] == "cycle_hub_4096" and h["variant"] == "standard")
+    data = np.fromfile(out, np.int32)
+    pos, got, prev = 1, [], 0
+    for level in range(int(data[0])):
+        n, m = int(data[pos]), int(data[pos + 1])
+        size = 2 + (n + 1) + 2 * m + n + (prev if level else 0)
+        got.append(hashlib.sha256(data[pos:pos + size].tobytes()).hexdigest())
+        pos += size
+        prev = n
+    assert got == [lv["sha256"] for lv in case["levels"]]
