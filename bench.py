@@ -260,6 +260,9 @@ def run_ours(args, rank, world, local, dist):
     ctx.partition_desc(ddesc, d_lab.data_ptr(), opts)
     prof = ctx.profile_dump()
     ctx.profile(False)
+    if args.profile_out is not None and rank == 0:
+        args.profile_out.parent.mkdir(parents=True, exist_ok=True)
+        args.profile_out.write_text(json.dumps(prof, indent=1, sort_keys=True))
     hbm, src_peak = peaks()
     result = None
     if rank == 0:
@@ -346,6 +349,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22_k32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-out", type=Path, default=None, help="write the full per-kernel profile (JSON)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     dist = Dist(world)

@@ -5,10 +5,13 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
+
 #include <cstdint>
 #include <cstring>
 #include <cstdio>
 #include <map>
+#include <unordered_map>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -39,6 +42,8 @@ struct Error : std::runtime_error {
 };
 [[noreturn]] inline void fail(gp_status s, const std::string& what) { throw Error(s, what); }
 
+struct Device;
+
 #define GP_CUDA(call)                                                              \
     do {                                                                           \
         const cudaError_t e__ = (call);                                            \
@@ -65,28 +70,81 @@ enum DeviceError : u32 {
 };
 
 // ---------------------------------------------------------------------------
-// Stream-ordered device allocation from a per-context memory pool that keeps
-// freed blocks cached (release threshold = UINT64_MAX), so repeated
-// partitions in one context allocate without touching the driver.
+// Device memory: a caching allocator per context.  Blocks are cudaMalloc'd in
+// size classes (<= 12.5% rounding) and kept on free lists when released.
+// All of a context's work runs on its one stream, so a released block can be
+// handed to the next allocation immediately: later work on the stream is
+// ordered after every earlier use.  Repeated partitions of similar graphs
+// therefore allocate nothing from the driver.
 // ---------------------------------------------------------------------------
 struct Device {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaMemPool_t pool = nullptr;
     int sms = 148;
     u32* err = nullptr;         // device error word
     void* pinned = nullptr;     // small pinned host staging area
     static constexpr size_t kPinnedBytes = 1 << 16;
 
+    std::map<size_t, std::vector<void*>> free_blocks;
+    std::unordered_map<void*, size_t> live;
+    size_t cached_bytes = 0, live_bytes = 0;
+    u64 alloc_calls = 0, driver_allocs = 0;
+    double alloc_ms = 0.0;   // host time spent inside the allocator
+
+    static size_t size_class(size_t bytes) {
+        if (bytes <= 4096) return (bytes + 255) & ~size_t{255};
+        int b = 0;
+        for (size_t x = bytes; x; x >>= 1) ++b;
+        const size_t q = size_t{1} << (b - 4);
+        return (bytes + q - 1) / q * q;
+    }
+    void release_cached() {
+        if (cached_bytes == 0) return;
+        cudaStreamSynchronize(stream);
+        for (auto& kv : free_blocks)
+            for (void* p : kv.second) cudaFree(p);
+        free_blocks.clear();
+        cached_bytes = 0;
+    }
     void* alloc(size_t bytes) {
         if (bytes == 0) return nullptr;
+        const auto t0 = std::chrono::steady_clock::now();
+        const size_t c = size_class(bytes);
         void* p = nullptr;
-        GP_CUDA(cudaMallocFromPoolAsync(&p, (bytes + 255) & ~size_t{255}, pool, stream));
+        auto it = free_blocks.find(c);
+        if (it != free_blocks.end() && !it->second.empty()) {
+            p = it->second.back();
+            it->second.pop_back();
+            cached_bytes -= c;
+        } else {
+            cudaError_t e = cudaMalloc(&p, c);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                release_cached();
+                e = cudaMalloc(&p, c);
+            }
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw_oom(c);
+            }
+            ++driver_allocs;
+        }
+        live[p] = c;
+        live_bytes += c;
+        ++alloc_calls;
+        alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return p;
     }
     void release(void* p) {
-        if (p) cudaFreeAsync(p, stream);
+        if (!p) return;
+        auto it = live.find(p);
+        if (it == live.end()) return;
+        free_blocks[it->second].push_back(p);
+        cached_bytes += it->second;
+        live_bytes -= it->second;
+        live.erase(it);
     }
+    [[noreturn]] static void throw_oom(size_t bytes);
     void sync() { GP_CUDA(cudaStreamSynchronize(stream)); }
     // Read a device error word; throws on any set bit.
     void check_errors();
@@ -146,6 +204,10 @@ void launch(Device& d, const char* name, void (*k)(KArgs...), dim3 grid, dim3 bl
         e.pending.push_back({a, b});
         ++e.launches;
     }
+}
+
+inline void Device::throw_oom(size_t bytes) {
+    fail(GP_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
 }
 
 template <typename T>

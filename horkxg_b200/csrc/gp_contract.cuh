@@ -16,6 +16,7 @@
 #pragma once
 
 #include "gp_prim.cuh"
+#include "gp_sclp.cuh"
 
 namespace gp {
 
@@ -31,8 +32,10 @@ __global__ void row_fine_degree_kernel(i64 n, const O* off, const i32* map, i64*
 }
 
 // Warp handles 32 consecutive fine rows: reserves each row's slot range in
-// its coarse segment, then walks the rows' contiguous edge range 32 entries
-// at a time; a lane finds its source row by a 5-step shuffle binary search.
+// its coarse segment, then walks the rows' edges 32 at a time in a virtual
+// position space (exclusive prefix of the rows' degrees); a lane finds its
+// row by a 5-step shuffle binary search.  Hub rows (degree > kHubDegree) are
+// reserved and scattered by the chunked hub kernels instead.
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) scatter_edges_kernel(
     i64 n, const O* __restrict__ off, const i32* __restrict__ nbr, const W* __restrict__ ew,
@@ -44,36 +47,52 @@ __global__ void __launch_bounds__(kThreads) scatter_edges_kernel(
     const i64 v = v0 + lane;
     const bool has = v < n;
     const i64 rs = has ? static_cast<i64>(off[v]) : 0;
-    const i64 re = has ? static_cast<i64>(off[v + 1]) : 0;
+    i64 deg = has ? static_cast<i64>(off[v + 1]) - rs : 0;
+    if (deg > kHubDegree) deg = 0;
     const i32 c = has ? map[v] : 0;
     i64 dst = 0;
-    if (has && re > rs)
+    if (deg > 0)
         dst = temp_off[c] + static_cast<i64>(atomicAdd(reinterpret_cast<unsigned long long*>(&cursor[c]),
-                                                        static_cast<unsigned long long>(re - rs)));
-    const i64 first = __shfl_sync(0xffffffffu, rs, 0);
-    i64 last = has ? re : 0;
-    for (int o = 16; o; o >>= 1) { const i64 x = __shfl_xor_sync(0xffffffffu, last, o); last = x > last ? x : last; }
-    for (i64 base = first; base < last; base += 32) {
-        const i64 e = base + lane;
-        // largest lane j with rs_j <= e (rows with rs_j == re_j are skipped
-        // naturally because a later row starts at the same offset)
+                                                        static_cast<unsigned long long>(deg)));
+    const i64 inc = warp_inclusive_sum(deg);
+    const i64 pre = inc - deg;
+    const i64 total = __shfl_sync(0xffffffffu, inc, 31);
+    for (i64 base = 0; base < total; base += 32) {
+        const i64 q = base + lane;
         int lo = 0;
 #pragma unroll
         for (int step = 16; step; step >>= 1) {
-            const i64 probe = __shfl_sync(0xffffffffu, rs, lo + step);
-            const bool probe_valid = v0 + lo + step < n;
-            if (probe_valid && probe <= e) lo += step;
+            const i64 probe = __shfl_sync(0xffffffffu, pre, lo + step);
+            if (probe <= q) lo += step;
         }
+        // lanes past the last non-empty row have pre == total > q, so `lo`
+        // is the last row starting at or before q, which is non-empty
+        const i64 my_pre = __shfl_sync(0xffffffffu, pre, lo);
         const i64 my_rs = __shfl_sync(0xffffffffu, rs, lo);
         const i64 my_dst = __shfl_sync(0xffffffffu, dst, lo);
         const i32 my_c = __shfl_sync(0xffffffffu, c, lo);
-        if (e < last) {
+        if (q < total) {
+            const i64 e = my_rs + (q - my_pre);
             const i32 t = map[nbr[e]];
-            const i64 out = my_dst + (e - my_rs);
+            const i64 out = my_dst + (q - my_pre);
             tgt[out] = t == my_c ? sentinel : static_cast<u32>(t);
             wt[out] = weight_at(ew, e);
         }
     }
+}
+
+// Segment reservation of hub rows (hub_dst[h]).
+template <typename O>
+__global__ void hub_reserve_kernel(i64 hubs, const i32* __restrict__ hub_list, const O* __restrict__ off,
+                                   const i32* __restrict__ map, const i64* __restrict__ temp_off, i64* cursor,
+                                   i64* hub_dst) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= hubs) return;
+    const i32 v = hub_list[h];
+    const i32 c = map[v];
+    const i64 deg = static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]);
+    hub_dst[h] = temp_off[c] + static_cast<i64>(atomicAdd(reinterpret_cast<unsigned long long*>(&cursor[c]),
+                                                           static_cast<unsigned long long>(deg)));
 }
 
 // Sum runs of equal keys of a sorted segment (keys, vals)[0, count); the
@@ -256,8 +275,9 @@ struct BigRowLen {
     }
 };
 
-// Copy each row's unique entries from its segment to the final CSR; warp per
-// 32 rows with a shuffle binary search (as in scatter_edges_kernel).
+// Copy each row's unique entries from its segment to the final CSR; a warp
+// per 32 rows in a virtual position space as in scatter_edges_kernel.  Rows
+// whose segment exceeded kSegSmem are copied by copy_big_rows_kernel.
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64* __restrict__ temp_off,
                                                              const O* __restrict__ coff, const u32* __restrict__ tgt,
@@ -269,25 +289,41 @@ __global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64
     const i64 r = r0 + lane;
     const bool has = r < rows;
     const i64 ds = has ? static_cast<i64>(coff[r]) : 0;
-    const i64 de = has ? static_cast<i64>(coff[r + 1]) : 0;
+    i64 len = has ? static_cast<i64>(coff[r + 1]) - ds : 0;
     const i64 src = has ? temp_off[r] : 0;
-    const i64 first = __shfl_sync(0xffffffffu, ds, 0);
-    i64 last = has ? de : 0;
-    for (int o = 16; o; o >>= 1) { const i64 x = __shfl_xor_sync(0xffffffffu, last, o); last = x > last ? x : last; }
-    for (i64 base = first; base < last; base += 32) {
-        const i64 e = base + lane;
+    if (has && temp_off[r + 1] - src > kSegSmem) len = 0;
+    const i64 inc = warp_inclusive_sum(len);
+    const i64 pre = inc - len;
+    const i64 total = __shfl_sync(0xffffffffu, inc, 31);
+    for (i64 base = 0; base < total; base += 32) {
+        const i64 q = base + lane;
         int lo = 0;
 #pragma unroll
         for (int step = 16; step; step >>= 1) {
-            const i64 probe = __shfl_sync(0xffffffffu, ds, lo + step);
-            if (r0 + lo + step < rows && probe <= e) lo += step;
+            const i64 probe = __shfl_sync(0xffffffffu, pre, lo + step);
+            if (probe <= q) lo += step;
         }
+        const i64 my_pre = __shfl_sync(0xffffffffu, pre, lo);
         const i64 my_ds = __shfl_sync(0xffffffffu, ds, lo);
         const i64 my_src = __shfl_sync(0xffffffffu, src, lo);
-        if (e < last) {
-            nbr[e] = static_cast<i32>(tgt[my_src + (e - my_ds)]);
-            ew[e] = wt[my_src + (e - my_ds)];
+        if (q < total) {
+            nbr[my_ds + (q - my_pre)] = static_cast<i32>(tgt[my_src + (q - my_pre)]);
+            ew[my_ds + (q - my_pre)] = wt[my_src + (q - my_pre)];
         }
+    }
+}
+
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) copy_big_rows_kernel(const i32* __restrict__ list,
+                                                                 const i64* __restrict__ temp_off,
+                                                                 const O* __restrict__ coff,
+                                                                 const u32* __restrict__ tgt, const W* __restrict__ wt,
+                                                                 i32* __restrict__ nbr, W* __restrict__ ew) {
+    const i32 r = list[blockIdx.x];
+    const i64 ds = coff[r], len = static_cast<i64>(coff[r + 1]) - ds, src = temp_off[r];
+    for (i64 i = threadIdx.x; i < len; i += kThreads) {
+        nbr[ds + i] = static_cast<i32>(tgt[src + i]);
+        ew[ds + i] = wt[src + i];
     }
 }
 

@@ -1,0 +1,445 @@
+// Hub splitting.  Power-law graphs (RMAT) have vertices with 10^4-10^6
+// neighbours; one warp or block per such vertex serialises a whole kernel
+// behind the largest hub.  Every level therefore keeps a hub index: the
+// vertices of degree > kHubThreshold, each cut into chunks of kChunkEdges
+// edges.  Kernels that walk rows skip hubs in their per-vertex loops and
+// handle hub chunks in a separate launch (one block per chunk), combining the
+// per-hub partial results with atomics or a per-hub finalisation.
+#pragma once
+
+#include "gp_prim.cuh"
+#include "gp_sclp.cuh"
+#include "gp_refine.cuh"
+
+namespace gp {
+
+constexpr i64 kHubThreshold = 2048;   // the SCLP global-hash class boundary
+constexpr i64 kChunkEdges = 2048;
+
+struct Chunk {
+    i32 v;       // vertex
+    i32 hub;     // index in the hub list
+    i64 begin;   // edge range
+    i64 end;
+};
+
+template <typename O>
+__device__ __forceinline__ bool is_hub(const O* off, i64 v) {
+    return static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubThreshold;
+}
+
+template <typename O>
+struct HubFlag {
+    const O* off;
+    __device__ i64 operator()(i64 v) const { return is_hub(off, v) ? 1 : 0; }
+};
+
+template <typename O>
+struct HubChunkCount {
+    const O* off;
+    __device__ i64 operator()(i64 v) const {
+        const i64 d = static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]);
+        return d > kHubThreshold ? (d + kChunkEdges - 1) / kChunkEdges : 0;
+    }
+};
+
+template <typename O>
+__global__ void hub_fill_kernel(i64 n, const O* off, const i64* hub_pos, const i64* chunk_pos, i32* hubs,
+                                Chunk* chunks, i64* chunk_begin) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n || !is_hub(off, v)) return;
+    const i64 h = hub_pos[v];
+    hubs[h] = static_cast<i32>(v);
+    chunk_begin[h] = chunk_pos[v];
+    const i64 b = off[v], e = off[v + 1];
+    i64 c = chunk_pos[v];
+    for (i64 s = b; s < e; s += kChunkEdges, ++c)
+        chunks[c] = {static_cast<i32>(v), static_cast<i32>(h), s, s + kChunkEdges < e ? s + kChunkEdges : e};
+}
+
+// ---------------------------------------------------------------------------
+// SCLP affinity of hubs: chunked insertion into per-hub global tables with
+// warp-level pre-aggregation (__match_any_sync on the cluster id), then a
+// candidate pass over 2048-slot tiles (tables are power-of-two sized and at
+// least 8192 slots, so tiles never straddle two tables), then a per-hub
+// finalisation that merges the tiles and decodes the proposal.
+// ---------------------------------------------------------------------------
+// One 16-byte slot holds key and value, so an insert or a read touches one
+// sector; key 0 is empty (cluster c is stored as c + 1), so a table is
+// cleared by a memset.
+struct HubSlot {
+    u32 key;
+    u32 pad;
+    u64 val;
+};
+
+__device__ __forceinline__ void slot_insert(HubSlot* table, u32 mask, i32 c, u64 w, u32* err) {
+    const u32 key = static_cast<u32>(c) + 1;
+    u32 slot = mix32(static_cast<u32>(c)) & mask;
+    for (u32 probe = 0; probe <= mask; ++probe) {
+        const u32 found = atomicCAS(&table[slot].key, 0u, key);
+        if (found == 0u || found == key) {
+            atomic_add_u64(&table[slot].val, w);
+            return;
+        }
+        slot = (slot + 1) & mask;
+    }
+    set_error(err, kErrTableFull);
+}
+
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) hub_insert_kernel(
+    const Chunk* __restrict__ chunks, const i32* __restrict__ nbr, const W* __restrict__ ew,
+    const i32* __restrict__ clusters, RoundParams p, const i64* __restrict__ table_off, HubSlot* table, u32* err) {
+    const Chunk ch = chunks[blockIdx.x];
+    const int lane = threadIdx.x & 31;
+    const i64 t0 = table_off[ch.hub];
+    const u32 mask = static_cast<u32>(table_off[ch.hub + 1] - t0 - 1);
+    HubSlot* slots = table + t0;
+    for (i64 base = ch.begin; base < ch.end; base += kThreads) {
+        const i64 e = base + threadIdx.x;
+        i32 c = -1;
+        u64 w = 0;
+        if (e < ch.end) {
+            const i32 u = nbr[e];
+            if (u != ch.v) {
+                c = p.identity ? u : clusters[u];
+                w = static_cast<u64>(weight_at(ew, e));
+            }
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        u64 sum = 0;
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            const u64 pw = __shfl_sync(0xffffffffu, w, s);
+            if (peers & (1u << s)) sum += pw;
+        }
+        if (c >= 0 && lane == __ffs(peers) - 1) slot_insert(slots, mask, c, sum, err);
+    }
+}
+
+struct HubPartial { u64 current, best, tie; };
+
+constexpr i64 kSlotTile = 2048;
+
+template <typename W>
+__global__ void __launch_bounds__(kThreads) hub_candidates_kernel(
+    i64 hubs, const i32* __restrict__ hub_list, const i64* __restrict__ table_off, HubSlot* table,
+    const i32* __restrict__ clusters, RoundParams p, HubPartial* partials) {
+    __shared__ CandShared red;
+    __shared__ int hub_sh;
+    const i64 s0 = static_cast<i64>(blockIdx.x) * kSlotTile;
+    if (threadIdx.x == 0) {
+        i64 lo = 0, hi = hubs - 1;   // last hub with table_off <= s0
+        while (lo < hi) {
+            const i64 mid = (lo + hi + 1) >> 1;
+            if (table_off[mid] <= s0) lo = mid; else hi = mid - 1;
+        }
+        hub_sh = static_cast<int>(lo);
+    }
+    __syncthreads();
+    const int h = hub_sh;
+    const i32 v = hub_list[h];
+    const i32 source = p.identity ? v : clusters[v];
+    u64 current = 0, best = 0, tie = 0;
+    for (i64 s = s0 + threadIdx.x; s < s0 + kSlotTile; s += kThreads) {
+        const HubSlot slot = table[s];
+        if (slot.key) {
+            slot_candidate(static_cast<i32>(slot.key - 1), slot.val, static_cast<u32>(v), source, p, current, best, tie);
+            table[s] = {0u, 0u, 0ULL};
+        }
+    }
+    block_candidate_reduce(current, best, tie, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = {current, best, tie};
+}
+
+template <typename W>
+__global__ void hub_finalize_kernel(i64 hubs, const i32* __restrict__ hub_list, const i64* __restrict__ table_off,
+                                    const HubPartial* __restrict__ partials, const i32* __restrict__ clusters,
+                                    const W* __restrict__ vw, const u64* __restrict__ cw, RoundParams p, SclpOut out) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= hubs) return;
+    const i32 v = hub_list[h];
+    const i32 source = p.identity ? v : clusters[v];
+    u64 current = 0, best = 0, tie = 0;
+    for (i64 t = table_off[h] / kSlotTile; t < table_off[h + 1] / kSlotTile; ++t) {
+        const HubPartial q = partials[t];
+        current = q.current > current ? q.current : current;
+        if (better(q.best, q.tie, best, tie)) { best = q.best; tie = q.tie; }
+    }
+    decode_and_write(v, source, current, best, tie, p, vw, cw, out);
+}
+
+// ---------------------------------------------------------------------------
+// Refinement and cut over hub chunks
+// ---------------------------------------------------------------------------
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) hub_cut_kernel(const Chunk* __restrict__ chunks,
+                                                           const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                           const i32* __restrict__ labels, u64* out) {
+    __shared__ u64 sh[kWarps + 1];
+    const Chunk ch = chunks[blockIdx.x];
+    const i32 s = labels[ch.v];
+    u64 local = 0;
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads)
+        if (labels[nbr[e]] != s) local += static_cast<u64>(weight_at(ew, e));
+    local = block_sum(local, sh);
+    if (threadIdx.x == 0 && local) atomic_add_u64(out, local);
+}
+
+template <typename C>
+__global__ void zero_hub_rows_kernel(i64 hubs, const i32* hub_list, int k, C* cache) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < hubs * k) cache[static_cast<i64>(hub_list[i / k]) * k + i % k] = 0;
+}
+
+template <typename W, typename C>
+__global__ void __launch_bounds__(kThreads) hub_build_cache_kernel(const Chunk* __restrict__ chunks,
+                                                                   const i32* __restrict__ nbr,
+                                                                   const W* __restrict__ ew,
+                                                                   const i32* __restrict__ labels, int k, C* cache) {
+    __shared__ unsigned long long row[32];
+    const Chunk ch = chunks[blockIdx.x];
+    if (threadIdx.x < 32) row[threadIdx.x] = 0;
+    __syncthreads();
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const i32 u = nbr[e];
+        if (u != ch.v) atomicAdd(&row[labels[u]], static_cast<unsigned long long>(weight_at(ew, e)));
+    }
+    __syncthreads();
+    if (threadIdx.x < k && row[threadIdx.x]) cache_add(&cache[static_cast<i64>(ch.v) * k + threadIdx.x], row[threadIdx.x]);
+}
+
+// Partial priority corrections of hub proposers (incremental_priority_filter,
+// src/refine_incremental.cuh:48-67), summed per hub.
+template <typename W>
+__global__ void __launch_bounds__(kThreads) hub_filter_kernel(const Chunk* __restrict__ chunks,
+                                                              const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                              const i32* __restrict__ labels,
+                                                              const i32* __restrict__ targets,
+                                                              const i64* __restrict__ gains, long long* corr) {
+    __shared__ long long sh[kWarps + 1];
+    const Chunk ch = chunks[blockIdx.x];
+    const i32 v = ch.v;
+    const i32 t = targets[v];
+    if (t < 0) return;
+    const i32 s = labels[v];
+    const i64 g = gains[v];
+    long long local = 0;
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const i32 u = nbr[e];
+        if (u == v) continue;
+        const i32 tu = targets[u];
+        if (tu < 0) continue;
+        const i64 gu = gains[u];
+        if (!(gu > g || (gu == g && u < v))) continue;
+        const i32 lu = labels[u];
+        local += static_cast<long long>(weight_at(ew, e)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+    }
+    local = block_sum(local, sh);
+    if (threadIdx.x == 0 && local) atomicAdd(reinterpret_cast<unsigned long long*>(&corr[ch.hub]),
+                                             static_cast<unsigned long long>(local));
+}
+
+__global__ void hub_filter_finalize_kernel(i64 hubs, const i32* __restrict__ hub_list,
+                                           const i32* __restrict__ targets, const i64* __restrict__ gains,
+                                           long long* corr, unsigned char* flags, i32* movers, RefineCounters* ctr) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= hubs) return;
+    const i32 v = hub_list[h];
+    const long long c = corr[h];
+    corr[h] = 0;
+    if (targets[v] < 0 || gains[v] + c < 0) return;
+    flags[v] = 1;
+    const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
+    movers[slot] = v;
+}
+
+template <typename W, typename C>
+__global__ void __launch_bounds__(kThreads) hub_apply_kernel(const Chunk* __restrict__ chunks,
+                                                             const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                             const i32* __restrict__ labels,
+                                                             const i32* __restrict__ targets,
+                                                             const unsigned char* __restrict__ flags, int k,
+                                                             C* cache, RefineCounters* ctr) {
+    __shared__ long long sh[kWarps + 1];
+    const Chunk ch = chunks[blockIdx.x];
+    const i32 v = ch.v;
+    if (!flags[v]) return;
+    const i32 s = labels[v], t = targets[v];
+    long long gain = 0;
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const i32 u = nbr[e];
+        if (u == v) continue;
+        const u64 w = static_cast<u64>(weight_at(ew, e));
+        cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
+        cache_add(&cache[static_cast<i64>(u) * k + t], w);
+        const bool fu = flags[u] != 0;
+        if (!fu || u > v) {
+            const i32 lu = labels[u];
+            const i32 nn = fu ? targets[u] : lu;
+            gain += static_cast<long long>(w) * ((s != lu) - (t != nn));
+        }
+    }
+    gain = block_sum(gain, sh);
+    if (threadIdx.x == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta),
+                                            static_cast<unsigned long long>(gain));
+}
+
+// ---------------------------------------------------------------------------
+// Contraction scatter of hub rows: the row's segment base was reserved by the
+// warp pass (hub_dst[hub]).
+// ---------------------------------------------------------------------------
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) hub_scatter_kernel(const Chunk* __restrict__ chunks,
+                                                               const O* __restrict__ off,
+                                                               const i32* __restrict__ nbr,
+                                                               const W* __restrict__ ew, const i32* __restrict__ map,
+                                                               const i64* __restrict__ hub_dst, u32 sentinel,
+                                                               u32* __restrict__ tgt, W* __restrict__ wt) {
+    const Chunk ch = chunks[blockIdx.x];
+    const i32 c = map[ch.v];
+    const i64 base = hub_dst[ch.hub] - static_cast<i64>(off[ch.v]);
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const i32 t = map[nbr[e]];
+        tgt[base + e] = t == c ? sentinel : static_cast<u32>(t);
+        wt[base + e] = weight_at(ew, e);
+    }
+}
+
+}  // namespace gp
+
+namespace gp {
+
+// ---------------------------------------------------------------------------
+// Identity rounds on duplicate-free rows: every neighbour is its own cluster,
+// so a vertex's connection to cluster u is the weight of its single edge to u
+// (the reference's singleton fast path, src/coarsen.cu:306-330,1158-1170).
+// No table is needed; the best candidate is a max over edges.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void direct_candidate(i32 v, i32 u, u64 w, const RoundParams& p, u64& best, u64& tie) {
+    if (u == v) return;
+    if (p.filter && is_mover(u, p)) return;
+    const u64 t = tie_key(static_cast<u32>(v), u, p.tie_salt);
+    if (better(w, t, best, tie)) { best = w; tie = t; }
+}
+
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) affinity_direct_warp_kernel(
+    i64 count, const i32* __restrict__ list, const O* __restrict__ off, const i32* __restrict__ nbr,
+    const W* __restrict__ ew, const W* __restrict__ vw, const u64* __restrict__ cw, RoundParams p, SclpOut out) {
+    const int lane = threadIdx.x & 31;
+    const i64 gid = (static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    if (gid >= count) return;
+    const i32 v = list[gid];
+    u64 current = 0, best = 0, tie = 0;
+    for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32)
+        direct_candidate(v, nbr[e], static_cast<u64>(weight_at(ew, e)), p, best, tie);
+    group_reduce(current, best, tie, 32, 0xffffffffu);
+    if (lane == 0) decode_and_write(v, v, current, best, tie, p, vw, cw, out);
+}
+
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) affinity_direct_block_kernel(
+    i64 count, const i32* __restrict__ list, const O* __restrict__ off, const i32* __restrict__ nbr,
+    const W* __restrict__ ew, const W* __restrict__ vw, const u64* __restrict__ cw, RoundParams p, SclpOut out) {
+    __shared__ CandShared red;
+    const i32 v = list[blockIdx.x];
+    u64 current = 0, best = 0, tie = 0;
+    for (i64 e = static_cast<i64>(off[v]) + threadIdx.x; e < static_cast<i64>(off[v + 1]); e += kThreads)
+        direct_candidate(v, nbr[e], static_cast<u64>(weight_at(ew, e)), p, best, tie);
+    block_candidate_reduce(current, best, tie, red);
+    if (threadIdx.x == 0) decode_and_write(v, v, current, best, tie, p, vw, cw, out);
+}
+
+// Hubs: one partial per chunk, merged per hub by hub_chunk_finalize_kernel.
+template <typename W>
+__global__ void __launch_bounds__(kThreads) hub_direct_kernel(const Chunk* __restrict__ chunks,
+                                                              const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                              RoundParams p, HubPartial* partials) {
+    __shared__ CandShared red;
+    const Chunk ch = chunks[blockIdx.x];
+    u64 current = 0, best = 0, tie = 0;
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads)
+        direct_candidate(ch.v, nbr[e], static_cast<u64>(weight_at(ew, e)), p, best, tie);
+    block_candidate_reduce(current, best, tie, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = {current, best, tie};
+}
+
+template <typename W>
+__global__ void hub_chunk_finalize_kernel(i64 hubs, const i32* __restrict__ hub_list,
+                                          const i64* __restrict__ chunk_begin,
+                                          const HubPartial* __restrict__ partials, const i32* __restrict__ clusters,
+                                          const W* __restrict__ vw, const u64* __restrict__ cw, RoundParams p,
+                                          SclpOut out) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= hubs) return;
+    const i32 v = hub_list[h];
+    const i32 source = p.identity ? v : clusters[v];
+    u64 current = 0, best = 0, tie = 0;
+    for (i64 c = chunk_begin[h]; c < chunk_begin[h + 1]; ++c) {
+        const HubPartial q = partials[c];
+        current = q.current > current ? q.current : current;
+        if (better(q.best, q.tie, best, tie)) { best = q.best; tie = q.tie; }
+    }
+    decode_and_write(v, source, current, best, tie, p, vw, cw, out);
+}
+
+// Hub insertion with shared-memory pre-aggregation: a block first sums its
+// chunk per cluster in a 4096-slot shared table, then adds each distinct
+// cluster once to the hub's global table.
+constexpr int kChunkSlots = 4096;   // >= 2 * kChunkEdges
+
+template <typename O, typename W>
+__global__ void __launch_bounds__(kThreads) hub_insert_smem_kernel(
+    const Chunk* __restrict__ chunks, const i32* __restrict__ nbr, const W* __restrict__ ew,
+    const i32* __restrict__ clusters, RoundParams p, const i64* __restrict__ table_off, i32* table_keys,
+    u64* table_vals, u32* err) {
+    extern __shared__ unsigned char smem_raw[];
+    u64* svals = reinterpret_cast<u64*>(smem_raw);
+    i32* skeys = reinterpret_cast<i32*>(svals + kChunkSlots);
+    const Chunk ch = chunks[blockIdx.x];
+    for (int s = threadIdx.x; s < kChunkSlots; s += kThreads) { skeys[s] = -1; svals[s] = 0; }
+    __syncthreads();
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const i32 u = nbr[e];
+        if (u == ch.v) continue;
+        table_insert(skeys, svals, kChunkSlots - 1, p.identity ? u : clusters[u], static_cast<u64>(weight_at(ew, e)),
+                     err);
+    }
+    __syncthreads();
+    const i64 t0 = table_off[ch.hub];
+    const u32 mask = static_cast<u32>(table_off[ch.hub + 1] - t0 - 1);
+    for (int s = threadIdx.x; s < kChunkSlots; s += kThreads)
+        if (skeys[s] >= 0) table_insert(table_keys + t0, table_vals + t0, mask, skeys[s], svals[s], err);
+}
+
+// Level-0 check of the reference's sorted-unique flag (src/coarsen.cu:44-70):
+// rows strictly increasing.  Warp per non-hub row; hub rows by chunks.
+template <typename O>
+__global__ void __launch_bounds__(kThreads) unsorted_rows_kernel(i64 n, const O* __restrict__ off,
+                                                                 const i32* __restrict__ nbr, u32* flag) {
+    const int lane = threadIdx.x & 31;
+    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
+    bool bad = false;
+    for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); v < n; v += warps_total) {
+        const i64 b = off[v], e1 = off[v + 1];
+        if (e1 - b > kHubDegree) continue;
+        for (i64 e = b + 1 + lane; e < e1; e += 32) bad |= nbr[e] <= nbr[e - 1];
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, 1u);
+}
+
+template <typename O>
+__global__ void __launch_bounds__(kThreads) hub_unsorted_kernel(const Chunk* __restrict__ chunks,
+                                                                const O* __restrict__ off,
+                                                                const i32* __restrict__ nbr, u32* flag) {
+    const Chunk ch = chunks[blockIdx.x];
+    const i64 row_begin = off[ch.v];
+    bool bad = false;
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads)
+        if (e > row_begin) bad |= nbr[e] <= nbr[e - 1];
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1u);
+}
+
+}  // namespace gp

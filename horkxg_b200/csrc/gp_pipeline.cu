@@ -25,6 +25,7 @@
 #include "gp_contract.cuh"
 #include "gp_initial.cuh"
 #include "gp_refine.cuh"
+#include "gp_hub.cuh"
 
 namespace gp {
 
@@ -73,12 +74,88 @@ struct DGraph {
     bool unit_ew = true, unit_vw = true;
     const W* ewp() const { return unit_ew ? nullptr : ew.get(); }
     const W* vwp() const { return unit_vw ? nullptr : vw.get(); }
+    // hub index (vertices of degree > kHubThreshold, chunked), built on demand
+    struct Hubs {
+        bool built = false;
+        i64 count = 0, chunks = 0;
+        Buf<i32> list;
+        Buf<Chunk> chunk;
+        Buf<i64> chunk_begin;   // per hub, count + 1 entries
+    };
+    mutable Hubs hubs;
+    // rows free of duplicate neighbours: 1 yes, 0 no, -1 not yet checked
+    mutable int unique_rows = -1;
 };
+
+template <typename T>
+const typename DGraph<T>::Hubs& hub_index(Device& d, const DGraph<T>& g) {
+    auto& h = g.hubs;
+    if (h.built) return h;
+    using O = typename T::O;
+    const i64 n = g.n;
+    Buf<i64> hpos(d, static_cast<size_t>(n) + 1), cpos(d, static_cast<size_t>(n) + 1), tot(d, 2);
+    exclusive_scan<i64>(d, HubFlag<O>{g.off.get()}, hpos.get(), n, tot.get());
+    exclusive_scan<i64>(d, HubChunkCount<O>{g.off.get()}, cpos.get(), n, tot.get() + 1);
+    i64 t[2];
+    fetch(d, t, tot.get(), 2);
+    h.count = t[0];
+    h.chunks = t[1];
+    if (h.count) {
+        h.list = Buf<i32>(d, static_cast<size_t>(h.count));
+        h.chunk = Buf<Chunk>(d, static_cast<size_t>(h.chunks));
+        h.chunk_begin = Buf<i64>(d, static_cast<size_t>(h.count) + 1);
+        launch(d, "hub_fill_kernel", hub_fill_kernel<O>, blocks_for(n, kThreads), kThreads, 0, n, g.off.get(),
+               hpos.get(), cpos.get(), h.list.get(), h.chunk.get(), h.chunk_begin.get());
+        GP_CUDA(cudaMemcpyAsync(h.chunk_begin.get() + h.count, tot.get() + 1, sizeof(i64), cudaMemcpyDeviceToDevice,
+                                d.stream));
+    }
+    h.built = true;
+    return h;
+}
+
+// The reference's level-0 sortedness flag (src/coarsen.cu:44-70,1965): rows
+// strictly increasing, hence duplicate-free.  Contracted levels are
+// duplicate-free by construction.
+template <typename T>
+bool unique_rows(Device& d, const DGraph<T>& g) {
+    if (g.unique_rows >= 0) return g.unique_rows == 1;
+    using O = typename T::O;
+    Buf<u32> flag(d, 1);
+    flag.zero(d);
+    launch(d, "unsorted_rows_kernel", unsorted_rows_kernel<O>, stride_grid(d, g.n * 32), kThreads, 0, g.n, g.off.get(),
+           g.nbr.get(), flag.get());
+    const auto& hubs = hub_index(d, g);
+    if (hubs.count)
+        launch(d, "hub_unsorted_kernel", hub_unsorted_kernel<O>, static_cast<int>(hubs.chunks), kThreads, 0,
+               hubs.chunk.get(), g.off.get(), g.nbr.get(), flag.get());
+    u32 f = 0;
+    fetch(d, &f, flag.get(), 1);
+    g.unique_rows = f ? 0 : 1;
+    return g.unique_rows == 1;
+}
 
 struct Log {
     bool on = false;
     std::ostream& out = std::cout;
 };
+
+// Opt-in phase trace (environment variable GP_TRACE=1): synchronises the
+// stream at each mark and prints the wall time since the previous mark to
+// stderr.  For locating host stalls; off in normal runs.
+struct Trace {
+    bool on = std::getenv("GP_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point last = std::chrono::steady_clock::now();
+    void mark(Device& d, const char* what, long long a = -1) {
+        if (!on) return;
+        d.sync();
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "trace %-28s %8.3f ms", what, std::chrono::duration<double, std::milli>(now - last).count());
+        if (a >= 0) std::fprintf(stderr, " (%lld)", a);
+        std::fprintf(stderr, "\n");
+        last = std::chrono::steady_clock::now();
+    }
+};
+inline Trace& trace() { static Trace t; return t; }
 
 __global__ void iota_kernel(i64 n, i32* a) {
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -93,6 +170,7 @@ __global__ void widen_weights_kernel(i64 n, const W* vw, u64* out) {
 
 template <typename W>
 __global__ void sat_sum_kernel(i64 m, const W* w, u64* out) {
+    __shared__ u64 sh[kWarps];
     u64 s = 0;
     for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x) {
         const u64 x = static_cast<u64>(weight_at(w, i));
@@ -102,13 +180,19 @@ __global__ void sat_sum_kernel(i64 m, const W* w, u64* out) {
         const u64 x = __shfl_xor_sync(0xffffffffu, s, o);
         s = ~0ULL - s < x ? ~0ULL : s + x;
     }
-    if ((threadIdx.x & 31) == 0 && s) {
-        u64 prev = *reinterpret_cast<volatile u64*>(out);
-        while (true) {
-            const u64 next = ~0ULL - prev < s ? ~0ULL : prev + s;
-            const u64 seen = atomic_cas_u64(out, prev, next);
-            if (seen == prev) break;
-            prev = seen;
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s = 0;
+        for (int i = 0; i < kWarps; ++i) s = ~0ULL - s < sh[i] ? ~0ULL : s + sh[i];
+        if (s) {
+            u64 prev = *reinterpret_cast<volatile u64*>(out);
+            while (true) {
+                const u64 next = ~0ULL - prev < s ? ~0ULL : prev + s;
+                const u64 seen = atomic_cas_u64(out, prev, next);
+                if (seen == prev) break;
+                prev = seen;
+            }
         }
     }
 }
@@ -135,8 +219,9 @@ struct SclpWork {
     Buf<u32> tie, ccount;
     Buf<unsigned char> cls;
     Buf<i64> pos, flags, positions, table_off;
-    Buf<i32> table_keys;
-    Buf<u64> table_vals, scalars;
+    Buf<HubSlot> table;
+    Buf<u64> scalars;
+    Buf<HubPartial> partials;
     void ensure(Device& d, i64 n) {
         const size_t s = static_cast<size_t>(n) + 1;
         clusters.ensure(d, s); target.ensure(d, s); list.ensure(d, s); list_alt.ensure(d, s);
@@ -195,6 +280,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
            w.clist.get(), w.ccount.get(), sc + 8);
     GP_LAUNCH();
     radix_sort<u64, i32>(d, w.ckeys.get(), w.clist.get(), w.ckeys_alt.get(), w.clist_alt.get(), n, 0, 8);
+    trace().mark(d, "agg.classes_launched", level);
     u64 stats[16];
     u32 cnt[kClasses];
     to_host(d, stats, sc, 16);
@@ -208,20 +294,24 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     const i32* lists = w.clist.get();
     auto class_list = [&](int c) { return lists + class_off[c]; };
 
+    trace().mark(d, "agg.classes_fetched", level);
+    // hash-free affinity on identity rounds (rows without duplicates)
+    const bool direct_ok = unique_rows(d, g);
     // global hash tables for hubs
-    const i64 hubs = cnt[5];
+    const auto& hubs = hub_index(d, g);
+    if (hubs.count != static_cast<i64>(cnt[5])) fail(GP_ERUNTIME, "hub index disagrees with degree classes");
     i64 table_total = 0;
-    if (hubs > 0) {
-        w.table_off.ensure(d, static_cast<size_t>(hubs) + 1);
-        exclusive_scan<i64>(d, HubTableSize<O>{class_list(5), off, hubs}, w.table_off.get(), hubs + 1,
-                            reinterpret_cast<i64*>(sc + 4));
+    if (hubs.count > 0) {
+        w.table_off.ensure(d, static_cast<size_t>(hubs.count) + 1);
+        exclusive_scan<i64>(d, HubTableSize<O>{hubs.list.get(), off, hubs.count}, w.table_off.get(),
+                            hubs.count + 1, reinterpret_cast<i64*>(sc + 4));
         fetch(d, &table_total, reinterpret_cast<i64*>(sc + 4), 1);
-        w.table_keys.ensure(d, static_cast<size_t>(table_total));
-        w.table_vals.ensure(d, static_cast<size_t>(table_total));
-        GP_CUDA(cudaMemsetAsync(w.table_keys.get(), 0xff, table_total * sizeof(i32), d.stream));
-        GP_CUDA(cudaMemsetAsync(w.table_vals.get(), 0, table_total * sizeof(u64), d.stream));
+        w.partials.ensure(d, static_cast<size_t>(std::max<i64>(table_total / kSlotTile, hubs.chunks)));
+        w.table.ensure(d, static_cast<size_t>(table_total));
+        GP_CUDA(cudaMemsetAsync(w.table.get(), 0, table_total * sizeof(HubSlot), d.stream));
     }
 
+    trace().mark(d, "agg.hub_tables", level);
     i32* clusters = w.clusters.get();
     u64* cw = w.cw.get();
     launch(d, "iota_kernel", iota_kernel, blocks_for(n, kThreads), kThreads, 0, n, clusters);
@@ -250,24 +340,41 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         if (cnt[2])
             launch(d, "affinity_small_kernel", affinity_small_kernel<32, O, W>, blocks_for(static_cast<i64>(cnt[2]) * 32, kThreads), kThreads, 0, 
                 cnt[2], class_list(2), off, nbr, ew, vw, clusters, cw, p, so);
+        const bool direct = p.identity && direct_ok;
+        if (cnt[3] && direct)
+            launch(d, "affinity_direct_warp_kernel", affinity_direct_warp_kernel<O, W>,
+                   blocks_for(static_cast<i64>(cnt[3]) * 32, kThreads), kThreads, 0, static_cast<i64>(cnt[3]),
+                   class_list(3), off, nbr, ew, vw, cw, p, so);
+        if (cnt[4] && direct)
+            launch(d, "affinity_direct_block_kernel", affinity_direct_block_kernel<O, W>, static_cast<int>(cnt[4]),
+                   kThreads, 0, static_cast<i64>(cnt[4]), class_list(4), off, nbr, ew, vw, cw, p, so);
+        if (cnt[5] && direct) {
+            launch(d, "hub_direct_kernel", hub_direct_kernel<W>, static_cast<int>(hubs.chunks), kThreads, 0,
+                   hubs.chunk.get(), nbr, ew, p, w.partials.get());
+            launch(d, "hub_chunk_finalize_kernel", hub_chunk_finalize_kernel<W>, blocks_for(hubs.count, kThreads),
+                   kThreads, 0, hubs.count, hubs.list.get(), hubs.chunk_begin.get(), w.partials.get(), clusters, vw,
+                   cw, p, so);
+        }
+        if (direct) return;
         if (cnt[3])
             launch(d, "affinity_warp_hash_kernel", affinity_warp_hash_kernel<O, W>, blocks_for(cnt[3], kWarps), kThreads, 0, 
                 cnt[3], class_list(3), off, nbr, ew, vw, clusters, cw, p, so, d.err);
-        if (cnt[4]) {
-            static bool configured = false;
-            if (!configured) {
-                GP_CUDA(cudaFuncSetAttribute(affinity_block_hash_kernel<O, W>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kLargeSlots * 12));
-                configured = true;
-            }
-        }
+        if (cnt[4])
+            GP_CUDA(cudaFuncSetAttribute(affinity_block_hash_kernel<O, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kLargeSlots * 12));
+
         if (cnt[4])
             launch(d, "affinity_block_hash_kernel", affinity_block_hash_kernel<O, W>, static_cast<int>(cnt[4]), kThreads, kLargeSlots * 12, 
                 cnt[4], class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
-        if (cnt[5])
-            launch(d, "affinity_global_hash_kernel", affinity_global_hash_kernel<O, W>, static_cast<int>(cnt[5]), kThreads, 0, 
-                cnt[5], class_list(5), off, nbr, ew, vw, clusters, cw, p, so, w.table_off.get(), w.table_keys.get(),
-                w.table_vals.get(), d.err);
+        if (cnt[5]) {
+            launch(d, "hub_insert_kernel", hub_insert_kernel<O, W>, static_cast<int>(hubs.chunks), kThreads, 0,
+                   hubs.chunk.get(), nbr, ew, clusters, p, w.table_off.get(), w.table.get(), d.err);
+            launch(d, "hub_candidates_kernel", hub_candidates_kernel<W>, static_cast<int>(table_total / kSlotTile),
+                   kThreads, 0, hubs.count, hubs.list.get(), w.table_off.get(), w.table.get(), clusters, p,
+                   w.partials.get());
+            launch(d, "hub_finalize_kernel", hub_finalize_kernel<W>, blocks_for(hubs.count, kThreads), kThreads, 0,
+                   hubs.count, hubs.list.get(), w.table_off.get(), w.partials.get(), clusters, vw, cw, p, so);
+        }
         GP_LAUNCH();
     };
     // compaction of cls == 2 into list (ascending) + count and gain maximum
@@ -324,6 +431,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
                                                                                  clusters, cw);
         GP_LAUNCH();
         cluster_count = count_clusters();
+        trace().mark(d, "agg.round", round);
         ++rounds;
         if (log.on)
             log.out << "ml_gpu_sclp_round level=" << level << " round=" << round << " mover_fraction=" << fraction
@@ -374,6 +482,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         cluster_count = count_clusters();
     }
 
+    trace().mark(d, "agg.isolated_two_hop", level);
     // compaction
     Buf<i32> compact(d, static_cast<size_t>(n));
     exclusive_scan<i32>(d, NonEmpty{cw}, compact.get(), n, reinterpret_cast<i32*>(sc + 6));
@@ -388,6 +497,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     GP_LAUNCH();
     out.coarse_n = coarse_n;
     out.cap = cap;
+    trace().mark(d, "agg.compaction", level);
     if (log.on)
         log.out << "ml_gpu_sclp level=" << level << " fine_vertices=" << n << " coarse_vertices=" << coarse_n
                 << " contraction_ratio=" << static_cast<double>(coarse_n) / static_cast<double>(n) << " beta=" << beta
@@ -414,14 +524,24 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     GP_LAUNCH();
     exclusive_scan_array<i64>(d, fdeg.get(), temp_off.get(), coarse_n + 1);
     const u32 sentinel = static_cast<u32>(coarse_n);
+    trace().mark(d, "contract.rows", coarse_n);
     Buf<u32> tgt(d, static_cast<size_t>(std::max<i64>(m, 1)));
     Buf<W> wt(d, static_cast<size_t>(std::max<i64>(m, 1)));
     const i64 warps = (n + 31) / 32;
     d.prof_bytes("scatter_edges_kernel", static_cast<double>(n + 1) * sizeof(O) + n * (4.0 + 8 + 8) +
                                              static_cast<double>(m) * (4 + 4 + 4 + (g.ewp() ? sizeof(W) : 0) + sizeof(W)));
-    launch(d, "scatter_edges_kernel", scatter_edges_kernel<O, W>, blocks_for(warps * 32, kThreads), kThreads, 0, 
-        n, g.off.get(), g.nbr.get(), g.ewp(), map, temp_off.get(), cursor.get(), sentinel, tgt.get(), wt.get());
+    launch(d, "scatter_edges_kernel", scatter_edges_kernel<O, W>, blocks_for(warps * 32, kThreads), kThreads, 0, n,
+           g.off.get(), g.nbr.get(), g.ewp(), map, temp_off.get(), cursor.get(), sentinel, tgt.get(), wt.get());
+    const auto& hubs = hub_index(d, g);
+    if (hubs.count) {
+        Buf<i64> hub_dst(d, static_cast<size_t>(hubs.count));
+        launch(d, "hub_reserve_kernel", hub_reserve_kernel<O>, blocks_for(hubs.count, kThreads), kThreads, 0,
+               hubs.count, hubs.list.get(), g.off.get(), map, temp_off.get(), cursor.get(), hub_dst.get());
+        launch(d, "hub_scatter_kernel", hub_scatter_kernel<O, W>, static_cast<int>(hubs.chunks), kThreads, 0,
+               hubs.chunk.get(), g.off.get(), g.nbr.get(), g.ewp(), map, hub_dst.get(), sentinel, tgt.get(), wt.get());
+    }
     GP_LAUNCH();
+    trace().mark(d, "contract.scatter", m);
     // row classes
     Buf<u64> rk(d, static_cast<size_t>(coarse_n)), rk_alt(d, static_cast<size_t>(coarse_n));
     Buf<i32> rl(d, static_cast<size_t>(coarse_n)), rl_alt(d, static_cast<size_t>(coarse_n));
@@ -462,6 +582,7 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
             aw.get(), row_len.get());
         GP_LAUNCH();
     }
+    trace().mark(d, "contract.segments", rcnt[3]);
     out.n = coarse_n;
     out.off = Buf<O>(d, static_cast<size_t>(coarse_n) + 1);
     exclusive_scan<O>(d, RowLenToO<O>{row_len.get()}, out.off.get(), coarse_n + 1, reinterpret_cast<O*>(scal.get() + 1));
@@ -473,12 +594,17 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     out.unit_ew = false;
     if (out.m > 0) {
         d.prof_bytes("copy_rows_kernel", static_cast<double>(coarse_n) * (sizeof(O) + 8) + 2.0 * out.m * (4 + sizeof(W)));
-        launch(d, "copy_rows_kernel", copy_rows_kernel<O, W>, blocks_for(((coarse_n + 31) / 32) * 32, kThreads), kThreads, 0, 
-            coarse_n, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
+        launch(d, "copy_rows_kernel", copy_rows_kernel<O, W>, blocks_for(((coarse_n + 31) / 32) * 32, kThreads),
+               kThreads, 0, coarse_n, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
+        if (rcnt[3])
+            launch(d, "copy_big_rows_kernel", copy_big_rows_kernel<O, W>, static_cast<int>(rcnt[3]), kThreads, 0,
+                   rl.get() + c3, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
         GP_LAUNCH();
     }
     out.vw = std::move(cvw);
     out.unit_vw = false;
+    out.unique_rows = 1;
+    trace().mark(d, "contract.copy", out.m);
 }
 
 // ---------------------------------------------------------------------------
@@ -672,8 +798,14 @@ void initial_partition(Device& d, const DGraph<T>& g, int parts, double ratio, u
     Buf<u64> loads(d, static_cast<size_t>(parts) + 1);
     loads.zero(d);
     launch(d, "part_weight_kernel", part_weight_kernel<W>, blocks_for(n, kThreads), kThreads, 0, n, labels.get(), g.vwp(), loads.get());
-    launch(d, "cut_kernel", cut_kernel<typename T::O, W>, stride_grid(d, static_cast<i64>(n) * 32), kThreads, 0, 
-        n, g.off.get(), g.nbr.get(), g.ewp(), labels.get(), loads.get() + parts);
+    launch(d, "cut_kernel", cut_kernel<typename T::O, W>, stride_grid(d, static_cast<i64>(n) * 32), kThreads, 0, n,
+           g.off.get(), g.nbr.get(), g.ewp(), labels.get(), loads.get() + parts);
+    {
+        const auto& hubs = hub_index(d, g);
+        if (hubs.count)
+            launch(d, "hub_cut_kernel", hub_cut_kernel<typename T::O, W>, static_cast<int>(hubs.chunks), kThreads, 0,
+                   hubs.chunk.get(), g.nbr.get(), g.ewp(), labels.get(), loads.get() + parts);
+    }
     GP_LAUNCH();
     std::vector<u64> host(static_cast<size_t>(parts) + 1);
     fetch(d, host.data(), loads.get(), host.size());
@@ -699,8 +831,12 @@ u64 directed_cut(Device& d, const DGraph<T>& g, const i32* labels, u64* scratch)
     GP_CUDA(cudaMemsetAsync(scratch, 0, sizeof(u64), d.stream));
     d.prof_bytes("cut_kernel", static_cast<double>(g.n + 1) * sizeof(typename T::O) + g.n * 4.0 +
                                    static_cast<double>(g.m) * (4 + 4 + (g.ewp() ? sizeof(typename T::W) : 0)));
-    launch(d, "cut_kernel", cut_kernel<typename T::O, typename T::W>, stride_grid(d, g.n * 32), kThreads, 0, 
-        g.n, g.off.get(), g.nbr.get(), g.ewp(), labels, scratch);
+    launch(d, "cut_kernel", cut_kernel<typename T::O, typename T::W>, stride_grid(d, g.n * 32), kThreads, 0, g.n,
+           g.off.get(), g.nbr.get(), g.ewp(), labels, scratch);
+    const auto& hubs = hub_index(d, g);
+    if (hubs.count)
+        launch(d, "hub_cut_kernel", hub_cut_kernel<typename T::O, typename T::W>, static_cast<int>(hubs.chunks),
+               kThreads, 0, hubs.chunk.get(), g.nbr.get(), g.ewp(), labels, scratch);
     GP_LAUNCH();
     u64 c = 0;
     fetch(d, &c, scratch, 1);
@@ -761,7 +897,18 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     d.prof_bytes("build_cache_kernel", static_cast<double>(n + 1) * sizeof(O) +
                                            static_cast<double>(g.m) * (4 + 4 + (ew ? sizeof(W) : 0)) +
                                            static_cast<double>(n) * k * sizeof(C));
-    launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr, ew, labels, k, cache);
+    launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr, ew,
+           labels, k, cache);
+    const auto& hubs = hub_index(d, g);
+    Buf<long long> hub_corr;
+    if (hubs.count) {
+        launch(d, "zero_hub_rows_kernel", zero_hub_rows_kernel<C>, blocks_for(hubs.count * k, kThreads), kThreads, 0,
+               hubs.count, hubs.list.get(), k, cache);
+        launch(d, "hub_build_cache_kernel", hub_build_cache_kernel<W, C>, static_cast<int>(hubs.chunks), kThreads, 0,
+               hubs.chunk.get(), nbr, ew, labels, k, cache);
+        hub_corr = Buf<long long>(d, static_cast<size_t>(hubs.count));
+        hub_corr.zero(d);
+    }
     GP_LAUNCH();
     u64 current_cut = undirected_cut(d, g, labels, w.scratch.get());
     st.initial_cut = current_cut;
@@ -787,8 +934,11 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     Buf<Stats> stats_dev(d, 1);
     auto finish_apply = [&](bool lp) -> i64 {
         // movers already listed in w.movers with counter ctr->movers
-        launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, 
-            w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
+        launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0,
+               w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
+        if (hubs.count)
+            launch(d, "hub_apply_kernel", hub_apply_kernel<W, C>, static_cast<int>(hubs.chunks), kThreads, 0,
+                   hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
         launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, n), kThreads, 0, w.movers.get(), ctr, labels, w.targets.get(), vw,
                                                                       pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
         GP_LAUNCH();
@@ -870,8 +1020,16 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         d.prof_bytes("lp_proposals_kernel", static_cast<double>(n) * (k * sizeof(C) + 4 + 1 + 4 + 8));
         launch(d, "lp_proposals_kernel", lp_proposals_kernel<C>, blocks_for(n, kThreads), kThreads, 0, 
             n, cache, labels, k, filter, w.locks.get(), w.targets.get(), w.gains.get(), w.list.get(), ctr);
-        launch(d, "priority_filter_kernel", priority_filter_kernel<O, W>, stride_grid(d, n * 32), kThreads, 0, 
-            w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.gains.get(), w.flags.get(), w.movers.get(), ctr);
+        launch(d, "priority_filter_kernel", priority_filter_kernel<O, W>, stride_grid(d, n * 32), kThreads, 0,
+               w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.gains.get(), w.flags.get(), w.movers.get(),
+               ctr);
+        if (hubs.count) {
+            launch(d, "hub_filter_kernel", hub_filter_kernel<W>, static_cast<int>(hubs.chunks), kThreads, 0,
+                   hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.gains.get(), hub_corr.get());
+            launch(d, "hub_filter_finalize_kernel", hub_filter_finalize_kernel, blocks_for(hubs.count, kThreads),
+                   kThreads, 0, hubs.count, hubs.list.get(), w.targets.get(), w.gains.get(), hub_corr.get(),
+                   w.flags.get(), w.movers.get(), ctr);
+        }
         GP_LAUNCH();
         const i64 count = finish_apply(true);
         st.proposals += static_cast<u64>(count);
@@ -1250,13 +1408,6 @@ gp_status gp_ctx_create(int device, gp_ctx** out) {
         GP_CUDA(cudaSetDevice(device));
         GP_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
         GP_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = device;
-        GP_CUDA(cudaMemPoolCreate(&d.pool, &props));
-        gp::u64 keep = UINT64_MAX;
-        GP_CUDA(cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep));
         GP_CUDA(cudaMalloc(&d.err, 64));
         GP_CUDA(cudaMemset(d.err, 0, 64));
         GP_CUDA(cudaMallocHost(&d.pinned, gp::Device::kPinnedBytes));
@@ -1274,9 +1425,12 @@ void gp_ctx_destroy(gp_ctx* ctx) {
     auto& d = ctx->dev;
     cudaSetDevice(d.device);
     if (d.stream) cudaStreamSynchronize(d.stream);
+    d.release_cached();
+    for (auto& kv : d.live) cudaFree(kv.first);
+    d.live.clear();
+    for (auto e : d.event_pool) cudaEventDestroy(e);
     if (d.err) cudaFree(d.err);
     if (d.pinned) cudaFreeHost(d.pinned);
-    if (d.pool) cudaMemPoolDestroy(d.pool);
     if (d.stream) cudaStreamDestroy(d.stream);
     delete ctx;
 }
@@ -1337,6 +1491,10 @@ gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* opt
             h.maps.clear();
             d.sync();
             const auto t4 = gp::Clock::now();
+            if (gp::trace().on)
+                std::fprintf(stderr, "trace allocations %llu calls (%llu from the driver), %.3f ms in the allocator\n",
+                             static_cast<unsigned long long>(d.alloc_calls),
+                             static_cast<unsigned long long>(d.driver_allocs), d.alloc_ms);
             rep.coarsen_seconds = std::chrono::duration<double>(t1 - t0).count();
             rep.initial_seconds = std::chrono::duration<double>(t2 - t1).count();
             rep.uncoarsen_seconds = std::chrono::duration<double>(t3 - t2).count();

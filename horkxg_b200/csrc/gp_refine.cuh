@@ -15,6 +15,7 @@
 #pragma once
 
 #include "gp_prim.cuh"
+#include "gp_sclp.cuh"
 
 namespace gp {
 
@@ -42,8 +43,10 @@ __global__ void __launch_bounds__(kThreads) cut_kernel(i64 n, const O* __restric
     u64 local = 0;
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
     for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); v < n; v += warps_total) {
+        const i64 b = off[v], end = off[v + 1];
+        if (end - b > kHubDegree) continue;   // hub rows: chunked kernel
         const i32 s = labels[v];
-        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32)
+        for (i64 e = b + lane; e < end; e += 32)
             if (labels[nbr[e]] != s) local += static_cast<u64>(weight_at(ew, e));
     }
     local = block_sum(local, sh);
@@ -59,6 +62,7 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
     for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + warp; v < n; v += warps_total) {
+        if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub rows: chunked kernel
         rows[warp][lane] = 0;
         __syncwarp();
         for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
@@ -113,6 +117,7 @@ __global__ void __launch_bounds__(kThreads) priority_filter_kernel(
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
     for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
         const i32 v = list[i];
+        if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub: chunked kernel
         const i32 s = labels[v], t = targets[v];
         const i64 g = gains[v];
         long long corr = 0;
@@ -149,6 +154,7 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
     long long gain = 0;
     for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
         const i32 v = movers[i];
+        if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub: chunked kernel
         const i32 s = labels[v], t = targets[v];
         for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
             const i32 u = nbr[e];

@@ -240,20 +240,22 @@ __global__ void __launch_bounds__(kThreads) affinity_block_hash_kernel(
     __shared__ CandShared red;
     const i64 gid = blockIdx.x;
     if (gid >= count) return;
-    for (int s = threadIdx.x; s < kLargeSlots; s += kThreads) { keys[s] = -1; vals[s] = 0; }
-    __syncthreads();
     const i32 v = list[gid];
     const i64 begin = off[v], end = off[v + 1];
+    int slots = 512;   // power of two >= 2 * degree (degree <= kHubDegree)
+    while (slots < 2 * (end - begin) && slots < kLargeSlots) slots <<= 1;
+    for (int s = threadIdx.x; s < slots; s += kThreads) { keys[s] = -1; vals[s] = 0; }
+    __syncthreads();
     for (i64 e = begin + threadIdx.x; e < end; e += kThreads) {
         const i32 u = nbr[e];
         if (u == v) continue;
-        table_insert(keys, vals, kLargeSlots - 1, p.identity ? u : clusters[u],
+        table_insert(keys, vals, static_cast<u32>(slots - 1), p.identity ? u : clusters[u],
                      static_cast<u64>(weight_at(ew, e)), err);
     }
     __syncthreads();
     const i32 source = p.identity ? v : clusters[v];
     u64 current = 0, best = 0, tie = 0;
-    for (int s = threadIdx.x; s < kLargeSlots; s += kThreads) slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
+    for (int s = threadIdx.x; s < slots; s += kThreads) slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
     block_candidate_reduce(current, best, tie, red);
     if (threadIdx.x == 0) decode_and_write(v, source, current, best, tie, p, vw, cw, out);
 }
@@ -331,8 +333,11 @@ struct HubTableSize {
         if (i >= count) return 0;
         const i32 v = list[i];
         const i64 d = static_cast<i64>(off[v + 1]) - off[v];
-        i64 s = 1;
-        while (s < 2 * d) s <<= 1;
+        // power of two >= 1.25 * degree, at least 4096 (a multiple of the
+        // 2048-slot candidate tile); rounds after the first see far fewer
+        // distinct clusters than neighbours
+        i64 s = 4096;
+        while (s < d + d / 4) s <<= 1;
         return s;
     }
 };

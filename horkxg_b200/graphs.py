@@ -104,6 +104,7 @@ def by_name(name: str) -> tuple[Path, Path]:
         "rmat12": lambda: rmat(12),
         "rmat14": lambda: rmat(14),
         "rmat16": lambda: rmat(16),
+        "rmat20": lambda: rmat(20),
         "rmat22": lambda: rmat(22),
         "rmat24": lambda: rmat(24),
         "rmat26": lambda: rmat(26),
