@@ -6,7 +6,7 @@
 //    into its coarse row's segment (internal edges become a sentinel);
 // 2. every segment is sorted by target and its runs of equal targets summed:
 //    a warp bitonic sort for segments of <= 32 entries, a shared-memory block
-//    radix sort for <= kSegSmem entries, a global-memory block radix sort for
+//    radix sort for segments that fit shared memory, a global-memory block radix sort for
 //    larger (hub) segments;
 // 3. row lengths are scanned into the coarse offsets and the unique entries
 //    copied out.
@@ -20,7 +20,10 @@
 
 namespace gp {
 
-constexpr int kSegSmem = 4096;
+// Largest segment sorted in shared memory: two key and two value buffers
+// (plus the ranking scratch) stay under the 227 KB a block may use.
+template <typename W>
+__host__ __device__ constexpr int seg_smem_capacity() { return 4096; }
 
 // Fine-degree sum per coarse row.
 template <typename O>
@@ -193,16 +196,18 @@ __global__ void __launch_bounds__(kThreads) segment_warp_kernel(i64 rows, const 
     if (lane == 0) row_len[c] = __popc(heads);
 }
 
-// Rows with 33..kSegSmem entries: block per row, radix sort in shared memory.
+// Rows with 33..seg_smem_capacity entries: block per row, radix sort in
+// shared memory.
 template <typename W>
 __global__ void __launch_bounds__(kThreads) segment_smem_kernel(i64 rows, const i32* __restrict__ list,
                                                                 const i64* __restrict__ temp_off, u32 sentinel,
                                                                 int key_bits, u32* tgt, W* wt, i64* row_len) {
     extern __shared__ unsigned char smem_raw[];
-    u32* k0 = reinterpret_cast<u32*>(smem_raw);
-    u32* k1 = k0 + kSegSmem;
-    W* w0 = reinterpret_cast<W*>(k1 + kSegSmem);
-    W* w1 = w0 + kSegSmem;
+    constexpr int cap = seg_smem_capacity<W>();
+    W* w0 = reinterpret_cast<W*>(smem_raw);
+    W* w1 = w0 + cap;
+    u32* k0 = reinterpret_cast<u32*>(w1 + cap);
+    u32* k1 = k0 + cap;
     __shared__ RankShared rank_sh;
     __shared__ RunShared<W> run_sh;
     const i64 r = blockIdx.x;
@@ -241,15 +246,15 @@ __global__ void __launch_bounds__(kThreads) segment_global_kernel(i64 rows, cons
     if (threadIdx.x == 0) row_len[c] = u;
 }
 
-// Row-size classes: 0 empty, 1 <= 32, 2 <= kSegSmem, 3 larger.
-__global__ void row_class_kernel(i64 rows, const i64* temp_off, u64* keys, i32* vals, u32* counts) {
+// Row-size classes: 0 empty, 1 <= 32, 2 <= smem_cap, 3 larger.
+__global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u64* keys, i32* vals, u32* counts) {
     __shared__ u32 local[4];
     if (threadIdx.x < 4) local[threadIdx.x] = 0;
     __syncthreads();
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c < rows) {
         const i64 l = temp_off[c + 1] - temp_off[c];
-        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kSegSmem ? 2 : 3;
+        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= smem_cap ? 2 : 3;
         keys[c] = static_cast<u64>(k);
         vals[c] = static_cast<i32>(c);
         atomicAdd(&local[k], 1u);
@@ -277,7 +282,8 @@ struct BigRowLen {
 
 // Copy each row's unique entries from its segment to the final CSR; a warp
 // per 32 rows in a virtual position space as in scatter_edges_kernel.  Rows
-// whose segment exceeded kSegSmem are copied by copy_big_rows_kernel.
+// whose segment exceeded the shared-memory capacity are copied by
+// copy_big_rows_kernel.
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64* __restrict__ temp_off,
                                                              const O* __restrict__ coff, const u32* __restrict__ tgt,
@@ -291,7 +297,7 @@ __global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64
     const i64 ds = has ? static_cast<i64>(coff[r]) : 0;
     i64 len = has ? static_cast<i64>(coff[r + 1]) - ds : 0;
     const i64 src = has ? temp_off[r] : 0;
-    if (has && temp_off[r + 1] - src > kSegSmem) len = 0;
+    if (has && temp_off[r + 1] - src > seg_smem_capacity<W>()) len = 0;
     const i64 inc = warp_inclusive_sum(len);
     const i64 pre = inc - len;
     const i64 total = __shfl_sync(0xffffffffu, inc, 31);

@@ -198,16 +198,34 @@ __global__ void __launch_bounds__(kThreads) hub_build_cache_kernel(const Chunk* 
                                                                    const i32* __restrict__ nbr,
                                                                    const W* __restrict__ ew,
                                                                    const i32* __restrict__ labels, int k, C* cache) {
-    __shared__ unsigned long long row[32];
+    __shared__ u64 rows[kWarps][32];
     const Chunk ch = chunks[blockIdx.x];
-    if (threadIdx.x < 32) row[threadIdx.x] = 0;
-    __syncthreads();
-    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
-        const i32 u = nbr[e];
-        if (u != ch.v) atomicAdd(&row[labels[u]], static_cast<unsigned long long>(weight_at(ew, e)));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    rows[warp][lane] = 0;
+    __syncwarp();
+    // each warp walks its own contiguous slice of the chunk
+    const i64 len = ch.end - ch.begin;
+    const i64 per = (len + kWarps - 1) / kWarps;
+    const i64 lo = ch.begin + warp * per, hi = lo + per < ch.end ? lo + per : ch.end;
+    for (i64 base = lo; base < hi; base += 32) {
+        const i64 e = base + lane;
+        int p = -1;
+        u64 w = 0;
+        if (e < hi) {
+            const i32 u = nbr[e];
+            if (u != ch.v) { p = labels[u]; w = static_cast<u64>(weight_at(ew, e)); }
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, p);
+        const u64 sum = group_sum<C>(peers, w);
+        if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][p] += sum;
+        __syncwarp();
     }
     __syncthreads();
-    if (threadIdx.x < k && row[threadIdx.x]) cache_add(&cache[static_cast<i64>(ch.v) * k + threadIdx.x], row[threadIdx.x]);
+    if (threadIdx.x < k) {
+        u64 t = 0;
+        for (int w2 = 0; w2 < kWarps; ++w2) t += rows[w2][threadIdx.x];
+        if (t) cache_add(&cache[static_cast<i64>(ch.v) * k + threadIdx.x], t);
+    }
 }
 
 // Partial priority corrections of hub proposers (incremental_priority_filter,
@@ -215,33 +233,32 @@ __global__ void __launch_bounds__(kThreads) hub_build_cache_kernel(const Chunk* 
 template <typename W>
 __global__ void __launch_bounds__(kThreads) hub_filter_kernel(const Chunk* __restrict__ chunks,
                                                               const i32* __restrict__ nbr, const W* __restrict__ ew,
-                                                              const i32* __restrict__ labels,
-                                                              const i32* __restrict__ targets,
-                                                              const i64* __restrict__ gains, long long* corr) {
+                                                              const PropRec* __restrict__ props, long long* corr) {
     __shared__ long long sh[kWarps + 1];
     const Chunk ch = chunks[blockIdx.x];
     const i32 v = ch.v;
-    const i32 t = targets[v];
+    const PropRec me = props[v];
+    const i32 t = me.target;
     if (t < 0) return;
-    const i32 s = labels[v];
-    const i64 g = gains[v];
+    const i32 s = me.label;
+    const i64 g = me.gain;
     long long local = 0;
     for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
         const i32 u = nbr[e];
         if (u == v) continue;
-        const i32 tu = targets[u];
-        if (tu < 0) continue;
-        const i64 gu = gains[u];
-        if (!(gu > g || (gu == g && u < v))) continue;
-        const i32 lu = labels[u];
-        local += static_cast<long long>(weight_at(ew, e)) * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+        const PropRec o = props[u];
+        if (o.target < 0) continue;
+        if (!(o.gain > g || (o.gain == g && u < v))) continue;
+        local += static_cast<long long>(weight_at(ew, e)) *
+                 ((o.target == t) - (o.target == s) - (o.label == t) + (o.label == s));
     }
     local = block_sum(local, sh);
     if (threadIdx.x == 0 && local) atomicAdd(reinterpret_cast<unsigned long long*>(&corr[ch.hub]),
                                              static_cast<unsigned long long>(local));
 }
 
-__global__ void hub_filter_finalize_kernel(i64 hubs, const i32* __restrict__ hub_list,
+template <typename O>
+__global__ void hub_filter_finalize_kernel(i64 hubs, const i32* __restrict__ hub_list, const O* __restrict__ off,
                                            const i32* __restrict__ targets, const i64* __restrict__ gains,
                                            long long* corr, unsigned char* flags, i32* movers, RefineCounters* ctr) {
     const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -253,6 +270,8 @@ __global__ void hub_filter_finalize_kernel(i64 hubs, const i32* __restrict__ hub
     flags[v] = 1;
     const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
     movers[slot] = v;
+    atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree),
+              static_cast<unsigned long long>(static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v])));
 }
 
 template <typename W, typename C>

@@ -96,6 +96,41 @@ __device__ void compute_norms(int tasks, const InitTask* task, const Moments* co
     }
 }
 
+// Rows longer than this are reduced by a whole block (fixed tree), shorter
+// ones by one warp, so the step time is not set by the densest row.
+constexpr i64 kHeavyRow = 512;
+
+// Sum over a row range of f(e) restricted to the group, with four
+// independent loads in flight per lane.  `stride` is the number of lanes
+// cooperating on the row (32 or kThreads).
+template <typename O, typename W, typename F>
+__device__ __forceinline__ float row_sum(i64 begin, i64 end, int lane, int stride, const i32* __restrict__ nbr,
+                                         const i32* __restrict__ labels, i32 group, const W* __restrict__ ew, F f) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    i64 e = begin + lane;
+    for (; e + 3 * stride < end; e += 4 * stride) {
+        const i32 u0 = nbr[e], u1 = nbr[e + stride], u2 = nbr[e + 2 * stride], u3 = nbr[e + 3 * stride];
+        const bool g0 = labels[u0] == group, g1 = labels[u1] == group, g2 = labels[u2] == group,
+                   g3 = labels[u3] == group;
+        if (g0) a0 += static_cast<float>(weight_at(ew, e)) * f(u0);
+        if (g1) a1 += static_cast<float>(weight_at(ew, e + stride)) * f(u1);
+        if (g2) a2 += static_cast<float>(weight_at(ew, e + 2 * stride)) * f(u2);
+        if (g3) a3 += static_cast<float>(weight_at(ew, e + 3 * stride)) * f(u3);
+    }
+    for (; e < end; e += stride) {
+        const i32 u = nbr[e];
+        if (labels[u] == group) a0 += static_cast<float>(weight_at(ew, e)) * f(u);
+    }
+    return (a0 + a1) + (a2 + a3);
+}
+
+struct One { __device__ float operator()(i32) const { return 1.f; } };
+struct Normalised {
+    const float* x;
+    float mean, scale;
+    __device__ float operator()(i32 u) const { return (x[u] - mean) * scale; }
+};
+
 // spectral_start + 64 x (normalize, spectral_step) + normalize
 // (src/initial_partition_gpu.cu:81-142,206-229) for all tasks of one depth.
 // x_out[v] receives the final normalised value; key[p] the sort key of
@@ -107,27 +142,38 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
     const i32* __restrict__ nbr, const W* __restrict__ ew, u32 seed, int steps, float* deg, float* xa, float* xb,
     Moments* contrib, float* x_out, u64* key, u32* bar_counter, u32* bar_gen, u32* err) {
     __shared__ NormShared sh;
+    __shared__ float red[kWarps + 1];
     const int lane = threadIdx.x & 31;
     const i32 warps_total = static_cast<i32>(gridDim.x) * kWarps;
     const i32 warp_id = static_cast<i32>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-    // start
-    for (i32 p = warp_id; p < positions; p += warps_total) {
+    // start: degree restricted to the group, x0 = hash, moment contributions
+    auto start_row = [&](i32 p, float d) {
+        const i32 v = order[p];
+        const i32 group = task[task_of_pos[p]].first_part;
+        const u32 h = mix32(static_cast<u32>(v) ^ (seed ^ static_cast<u32>(group)));
+        const float a = static_cast<float>(static_cast<double>(h) / 4294967296.0 - 0.5);
+        deg[v] = d;
+        xa[v] = a;
+        const float mass = d > 0.f ? d : 1.f;
+        contrib[p] = {mass, mass * a, mass * a * a};
+    };
+    for (i32 p = blockIdx.x; p < positions; p += gridDim.x) {   // heavy rows: block per row
         const i32 t = task_of_pos[p];
         if (t < 0) continue;
         const i32 v = order[p];
-        const i32 group = task[t].first_part;
-        float d = 0.f;
-        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32)
-            if (labels[nbr[e]] == group) d += static_cast<float>(weight_at(ew, e));
-        d = warp_sum(d);
-        if (lane == 0) {
-            const u32 h = mix32(static_cast<u32>(v) ^ (seed ^ static_cast<u32>(group)));
-            const float a = static_cast<float>(static_cast<double>(h) / 4294967296.0 - 0.5);
-            deg[v] = d;
-            xa[v] = a;
-            const float mass = d > 0.f ? d : 1.f;
-            contrib[p] = {mass, mass * a, mass * a * a};
-        }
+        const i64 b = off[v], e = off[v + 1];
+        if (e - b <= kHeavyRow) continue;
+        const float d = block_sum(row_sum<O, W>(b, e, threadIdx.x, kThreads, nbr, labels, task[t].first_part, ew, One{}), red);
+        if (threadIdx.x == 0) start_row(p, d);
+    }
+    for (i32 p = warp_id; p < positions; p += warps_total) {      // light rows: warp per row
+        const i32 t = task_of_pos[p];
+        if (t < 0) continue;
+        const i32 v = order[p];
+        const i64 b = off[v], e = off[v + 1];
+        if (e - b > kHeavyRow) continue;
+        const float d = warp_sum(row_sum<O, W>(b, e, lane, 32, nbr, labels, task[t].first_part, ew, One{}));
+        if (lane == 0) start_row(p, d);
     }
     float* x = xa;
     float* y = xb;
@@ -135,26 +181,34 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
         grid_barrier(bar_counter, bar_gen, err);
         compute_norms(tasks, task, contrib, sh);
         if (it == steps) break;
+        auto step_row = [&](i32 p, i32 t, float s) {
+            const i32 v = order[p];
+            const float d = deg[v];
+            const float xv = (x[v] - sh.mean[t]) * sh.scale[t];
+            const float a = d > 0.f ? 0.5f * (xv + s / d) : xv;
+            y[v] = a;
+            const float mass = d > 0.f ? d : 1.f;
+            contrib[p] = {mass, mass * a, mass * a * a};
+        };
+        for (i32 p = blockIdx.x; p < positions; p += gridDim.x) {
+            const i32 t = task_of_pos[p];
+            if (t < 0) continue;
+            const i32 v = order[p];
+            const i64 b = off[v], e = off[v + 1];
+            if (e - b <= kHeavyRow) continue;
+            const float s = block_sum(row_sum<O, W>(b, e, threadIdx.x, kThreads, nbr, labels, task[t].first_part, ew,
+                                                    Normalised{x, sh.mean[t], sh.scale[t]}), red);
+            if (threadIdx.x == 0) step_row(p, t, s);
+        }
         for (i32 p = warp_id; p < positions; p += warps_total) {
             const i32 t = task_of_pos[p];
             if (t < 0) continue;
             const i32 v = order[p];
-            const i32 group = task[t].first_part;
-            const float mean = sh.mean[t], scale = sh.scale[t];
-            float s = 0.f;
-            for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
-                const i32 u = nbr[e];
-                if (labels[u] == group) s += static_cast<float>(weight_at(ew, e)) * ((x[u] - mean) * scale);
-            }
-            s = warp_sum(s);
-            if (lane == 0) {
-                const float d = deg[v];
-                const float xv = (x[v] - mean) * scale;
-                const float a = d > 0.f ? 0.5f * (xv + s / d) : xv;
-                y[v] = a;
-                const float mass = d > 0.f ? d : 1.f;
-                contrib[p] = {mass, mass * a, mass * a * a};
-            }
+            const i64 b = off[v], e = off[v + 1];
+            if (e - b > kHeavyRow) continue;
+            const float s = warp_sum(row_sum<O, W>(b, e, lane, 32, nbr, labels, task[t].first_part, ew,
+                                                   Normalised{x, sh.mean[t], sh.scale[t]}));
+            if (lane == 0) step_row(p, t, s);
         }
         float* tmp = x; x = y; y = tmp;
     }

@@ -221,6 +221,8 @@ struct SclpWork {
     Buf<i64> pos, flags, positions, table_off;
     Buf<HubSlot> table;
     Buf<u64> scalars;
+    u64 edge_total = 0;          // total directed edge weight of the first level (an upper bound below)
+    bool edge_total_known = false;
     Buf<HubPartial> partials;
     void ensure(Device& d, i64 n) {
         const size_t s = static_cast<size_t>(n) + 1;
@@ -295,6 +297,18 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     auto class_list = [&](int c) { return lists + class_off[c]; };
 
     trace().mark(d, "agg.classes_fetched", level);
+    if (!w.edge_total_known) {
+        if (ew) {
+            Buf<u64> t(d, 1);
+            t.zero(d);
+            launch(d, "sat_sum_kernel", sat_sum_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, ew, t.get());
+            fetch(d, &w.edge_total, t.get(), 1);
+        } else {
+            w.edge_total = static_cast<u64>(g.m);
+        }
+        w.edge_total_known = true;
+    }
+    const int sum32 = w.edge_total <= 0xffffffffULL ? 1 : 0;
     // hash-free affinity on identity rounds (rows without duplicates)
     const bool direct_ok = unique_rows(d, g);
     // global hash tables for hubs
@@ -408,7 +422,8 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         const i64 removable = std::max<i64>(0, cluster_count - desired);
         const double fraction = std::min(0.50, static_cast<double>(removable) / static_cast<double>(cluster_count));
         const auto threshold = static_cast<u32>(fraction * 4294967296.0);
-        const RoundParams p = make_round(seed, level, round, true, threshold);
+        RoundParams p = make_round(seed, level, round, true, threshold);
+        p.sum32 = sum32;
         w.demand.zero(d);
         affinity(p);
         GP_CUDA(cudaMemsetAsync(sc + 3, 0, sizeof(u64), d.stream));
@@ -456,6 +471,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     if (static_cast<double>(cluster_count) > 0.60 * n) {
         RoundParams p = make_round(seed, level, 4, false, 0);
         p.two_hop = 1;
+        p.sum32 = sum32;
         affinity(p);
         GP_CUDA(cudaMemsetAsync(sc + 3, 0, sizeof(u64), d.stream));
         launch(d, "favorite_classify_kernel", favorite_classify_kernel, blocks_for(n, kThreads), kThreads, 0, n, w.target.get(), w.gain.get(),
@@ -547,8 +563,8 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     Buf<i32> rl(d, static_cast<size_t>(coarse_n)), rl_alt(d, static_cast<size_t>(coarse_n));
     Buf<u32> rc(d, 4);
     rc.zero(d);
-    launch(d, "row_class_kernel", row_class_kernel, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n, temp_off.get(), rk.get(),
-                                                                              rl.get(), rc.get());
+    launch(d, "row_class_kernel", row_class_kernel, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n,
+           temp_off.get(), static_cast<i64>(seg_smem_capacity<W>()), rk.get(), rl.get(), rc.get());
     GP_LAUNCH();
     radix_sort<u64, i32>(d, rk.get(), rl.get(), rk_alt.get(), rl_alt.get(), coarse_n, 0, 8);
     u32 rcnt[4];
@@ -561,7 +577,7 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
         launch(d, "segment_warp_kernel", segment_warp_kernel<W>, blocks_for(static_cast<i64>(rcnt[1]) * 32, kThreads), kThreads, 0, 
             rcnt[1], rl.get() + c1, temp_off.get(), sentinel, tgt.get(), wt.get(), row_len.get());
     if (rcnt[2]) {
-        const size_t smem = 2 * kSegSmem * (sizeof(u32) + sizeof(W));
+        const size_t smem = 2 * static_cast<size_t>(seg_smem_capacity<W>()) * (sizeof(u32) + sizeof(W));
         GP_CUDA(cudaFuncSetAttribute(segment_smem_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         launch(d, "segment_smem_kernel", segment_smem_kernel<W>, static_cast<int>(rcnt[2]), kThreads, smem, 
@@ -854,6 +870,7 @@ struct RefineWork {
     Buf<unsigned char> cache_raw;
     Buf<i32> targets, list, movers, saved_labels, clist, clist_alt;
     Buf<i64> gains, pos;
+    Buf<PropRec> props;
     Buf<unsigned char> locks, flags;
     Buf<double> gpw;
     Buf<i32> bucket;
@@ -864,7 +881,7 @@ struct RefineWork {
         cache_raw.ensure(d, cache_bytes);
         targets.ensure(d, s); list.ensure(d, s); movers.ensure(d, s); saved_labels.ensure(d, s);
         clist.ensure(d, s); clist_alt.ensure(d, s);
-        gains.ensure(d, s); pos.ensure(d, s);
+        gains.ensure(d, s); pos.ensure(d, s); props.ensure(d, s);
         locks.ensure(d, s); flags.ensure(d, s);
         gpw.ensure(d, s); bucket.ensure(d, s);
         rank.ensure(d, s); excl.ensure(d, s); keys.ensure(d, s); keys_alt.ensure(d, s);
@@ -932,26 +949,51 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     const double filter = maxe <= 1 ? 0.25 : 0.75;
     struct Stats { RefineCounters c; u64 pw[32]; };
     Buf<Stats> stats_dev(d, 1);
+    auto build_cache = [&]() {
+        launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr,
+               ew, labels, k, cache);
+        if (hubs.count) {
+            launch(d, "zero_hub_rows_kernel", zero_hub_rows_kernel<C>, blocks_for(hubs.count * k, kThreads), kThreads,
+                   0, hubs.count, hubs.list.get(), k, cache);
+            launch(d, "hub_build_cache_kernel", hub_build_cache_kernel<W, C>, static_cast<int>(hubs.chunks), kThreads,
+                   0, hubs.chunk.get(), nbr, ew, labels, k, cache);
+        }
+    };
+    // Applies the listed movers.  When their edges outnumber m/8, updating the
+    // affinity cache edge by edge (two random atomics per edge) costs more
+    // than rebuilding it with one streaming pass, and the cut is then
+    // recounted exactly instead of being updated by the per-edge deltas; both
+    // routes give the same cache and the same cut.
     auto finish_apply = [&](bool lp) -> i64 {
-        // movers already listed in w.movers with counter ctr->movers
-        launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0,
-               w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
-        if (hubs.count)
-            launch(d, "hub_apply_kernel", hub_apply_kernel<W, C>, static_cast<int>(hubs.chunks), kThreads, 0,
-                   hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
-        launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, n), kThreads, 0, w.movers.get(), ctr, labels, w.targets.get(), vw,
-                                                                      pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
-        GP_LAUNCH();
+        RefineCounters c0;
+        fetch(d, &c0, ctr, 1);
+        if (c0.movers == 0) return 0;
+        const bool rebuild = lp && c0.mover_degree > g.m / 8;
+        if (!rebuild) {
+            launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, c0.movers * 32),
+                   kThreads, 0, w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache,
+                   ctr);
+            if (hubs.count)
+                launch(d, "hub_apply_kernel", hub_apply_kernel<W, C>, static_cast<int>(hubs.chunks), kThreads, 0,
+                       hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
+        }
+        launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, c0.movers), kThreads, 0, w.movers.get(), ctr, labels,
+               w.targets.get(), vw, pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
+        if (rebuild) build_cache();
         GP_CUDA(cudaMemcpyAsync(&stats_dev.get()->c, ctr, sizeof(RefineCounters), cudaMemcpyDeviceToDevice, d.stream));
         GP_CUDA(cudaMemcpyAsync(stats_dev.get()->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
         Stats h;
         fetch(d, &h, stats_dev.get(), 1);
-        const long long delta = h.c.delta;
-        if (delta >= 0) {
-            if (static_cast<u64>(delta) > current_cut) fail(GP_ERUNTIME, "incremental cut underflow");
-            current_cut -= static_cast<u64>(delta);
+        if (rebuild) {
+            current_cut = undirected_cut(d, g, labels, w.scratch.get());
         } else {
-            current_cut += static_cast<u64>(-delta);
+            const long long delta = h.c.delta;
+            if (delta >= 0) {
+                if (static_cast<u64>(delta) > current_cut) fail(GP_ERUNTIME, "incremental cut underflow");
+                current_cut -= static_cast<u64>(delta);
+            } else {
+                current_cut += static_cast<u64>(-delta);
+            }
         }
         std::copy(h.pw, h.pw + k, host_pw.begin());
         st.accepted += static_cast<u64>(h.c.movers);
@@ -1018,16 +1060,15 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         st.rounds = phase + 1;
         GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
         d.prof_bytes("lp_proposals_kernel", static_cast<double>(n) * (k * sizeof(C) + 4 + 1 + 4 + 8));
-        launch(d, "lp_proposals_kernel", lp_proposals_kernel<C>, blocks_for(n, kThreads), kThreads, 0, 
-            n, cache, labels, k, filter, w.locks.get(), w.targets.get(), w.gains.get(), w.list.get(), ctr);
+        launch(d, "lp_proposals_kernel", lp_proposals_kernel<C>, blocks_for(n, kThreads), kThreads, 0, n, cache, labels, k,
+               filter, w.locks.get(), w.targets.get(), w.gains.get(), w.props.get(), w.list.get(), ctr);
         launch(d, "priority_filter_kernel", priority_filter_kernel<O, W>, stride_grid(d, n * 32), kThreads, 0,
-               w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.gains.get(), w.flags.get(), w.movers.get(),
-               ctr);
+               w.list.get(), ctr, off, nbr, ew, w.props.get(), w.flags.get(), w.movers.get(), ctr);
         if (hubs.count) {
             launch(d, "hub_filter_kernel", hub_filter_kernel<W>, static_cast<int>(hubs.chunks), kThreads, 0,
-                   hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.gains.get(), hub_corr.get());
-            launch(d, "hub_filter_finalize_kernel", hub_filter_finalize_kernel, blocks_for(hubs.count, kThreads),
-                   kThreads, 0, hubs.count, hubs.list.get(), w.targets.get(), w.gains.get(), hub_corr.get(),
+                   hubs.chunk.get(), nbr, ew, w.props.get(), hub_corr.get());
+            launch(d, "hub_filter_finalize_kernel", hub_filter_finalize_kernel<O>, blocks_for(hubs.count, kThreads),
+                   kThreads, 0, hubs.count, hubs.list.get(), off, w.targets.get(), w.gains.get(), hub_corr.get(),
                    w.flags.get(), w.movers.get(), ctr);
         }
         GP_LAUNCH();

@@ -26,7 +26,16 @@ struct RefineCounters {
     i64 movers;
     long long delta;      // cut decrease of the last apply
     u64 directed_cut;
-    u64 pad[4];
+    i64 mover_degree;     // sum of the movers' degrees
+    u64 pad[3];
+};
+
+// Per-vertex proposal record written by the LP pass: the priority filter
+// gathers one 16-byte record per neighbour instead of three arrays.
+struct alignas(16) PropRec {
+    i32 label;
+    i32 target;   // -1: no proposal
+    i64 gain;
 };
 
 __device__ __forceinline__ void cache_add(u32* p, u64 v) { atomicAdd(p, static_cast<u32>(v)); }
@@ -53,7 +62,27 @@ __global__ void __launch_bounds__(kThreads) cut_kernel(i64 n, const O* __restric
     if (threadIdx.x == 0 && local) atomic_add_u64(out, local);
 }
 
-// incremental_build_affinity (src/refine_incremental.cuh:7-25)
+// Sum of `w` over the lanes that share this lane's `key` (the lanes of
+// `peers`), the same value in every lane of the group.
+template <typename C>
+__device__ __forceinline__ u64 group_sum(unsigned peers, u64 w) {
+    if constexpr (sizeof(C) == 4) {
+        return __reduce_add_sync(peers, static_cast<u32>(w));
+    } else {
+        u64 sum = 0;
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            const u64 x = __shfl_sync(0xffffffffu, w, s);
+            if (peers & (1u << s)) sum += x;
+        }
+        return sum;
+    }
+}
+
+// incremental_build_affinity (src/refine_incremental.cuh:7-25), warp per
+// vertex.  Lanes holding the same part are grouped with __match_any_sync and
+// only the group leader adds to the warp's private row, so the row needs no
+// atomics.
 template <typename O, typename W, typename C>
 __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* __restrict__ off,
                                                                const i32* __restrict__ nbr, const W* __restrict__ ew,
@@ -62,15 +91,23 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
     for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + warp; v < n; v += warps_total) {
-        if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub rows: chunked kernel
+        const i64 b = off[v], end = off[v + 1];
+        if (end - b > kHubDegree) continue;   // hub rows: chunked kernel
         rows[warp][lane] = 0;
         __syncwarp();
-        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
-            const i32 u = nbr[e];
-            if (u != v) atomicAdd(reinterpret_cast<unsigned long long*>(&rows[warp][labels[u]]),
-                                  static_cast<unsigned long long>(weight_at(ew, e)));
+        for (i64 base = b; base < end; base += 32) {
+            const i64 e = base + lane;
+            int p = -1;
+            u64 w = 0;
+            if (e < end) {
+                const i32 u = nbr[e];
+                if (u != v) { p = labels[u]; w = static_cast<u64>(weight_at(ew, e)); }
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, p);
+            const u64 sum = group_sum<C>(peers, w);
+            if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][p] += sum;
+            __syncwarp();
         }
-        __syncwarp();
         if (lane < k) cache[v * k + lane] = static_cast<C>(rows[warp][lane]);
         __syncwarp();
     }
@@ -80,14 +117,15 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
 // are appended to `list`.
 template <typename C>
 __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i32* __restrict__ labels, int k,
-                                    double filter, unsigned char* locks, i32* targets, i64* gains, i32* list,
-                                    RefineCounters* ctr) {
+                                    double filter, unsigned char* locks, i32* targets, i64* gains, PropRec* props,
+                                    i32* list, RefineCounters* ctr) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (v >= n) return;
     targets[v] = -1;
     gains[v] = INT64_MIN;
-    if (locks[v]) { locks[v] = 0; return; }
     const i32 s = labels[v];
+    props[v] = {s, -1, INT64_MIN};
+    if (locks[v]) { locks[v] = 0; return; }
     const C* row = cache + v * k;
     u64 best = 0;
     int target = -1;
@@ -97,8 +135,10 @@ __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i3
     }
     const u64 current = static_cast<u64>(row[s]);
     if (target >= 0 && (best >= current || current - best < static_cast<u64>(filter * static_cast<double>(current)))) {
+        const i64 g = best >= current ? static_cast<i64>(best - current) : -static_cast<i64>(current - best);
         targets[v] = target;
-        gains[v] = best >= current ? static_cast<i64>(best - current) : -static_cast<i64>(current - best);
+        gains[v] = g;
+        props[v] = {s, target, g};
         const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->proposers), 1ULL);
         list[slot] = static_cast<i32>(v);
     }
@@ -109,34 +149,34 @@ __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i3
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) priority_filter_kernel(
     const i32* __restrict__ list, const RefineCounters* ctr_in, const O* __restrict__ off,
-    const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
-    const i32* __restrict__ targets, const i64* __restrict__ gains, unsigned char* flags, i32* movers,
-    RefineCounters* ctr) {
+    const i32* __restrict__ nbr, const W* __restrict__ ew, const PropRec* __restrict__ props, unsigned char* flags,
+    i32* movers, RefineCounters* ctr) {
     const int lane = threadIdx.x & 31;
     const i64 count = ctr_in->proposers;
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
     for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
         const i32 v = list[i];
         if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub: chunked kernel
-        const i32 s = labels[v], t = targets[v];
-        const i64 g = gains[v];
+        const PropRec me = props[v];
+        const i32 s = me.label, t = me.target;
+        const i64 g = me.gain;
         long long corr = 0;
         for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
             const i32 u = nbr[e];
             if (u == v) continue;
-            const i32 tu = targets[u];
-            if (tu < 0) continue;
-            const i64 gu = gains[u];
-            if (!(gu > g || (gu == g && u < v))) continue;
-            const i32 lu = labels[u];
+            const PropRec o = props[u];
+            if (o.target < 0) continue;
+            if (!(o.gain > g || (o.gain == g && u < v))) continue;
             const auto w = static_cast<long long>(weight_at(ew, e));
-            corr += w * ((tu == t) - (tu == s) - (lu == t) + (lu == s));
+            corr += w * ((o.target == t) - (o.target == s) - (o.label == t) + (o.label == s));
         }
         corr = warp_sum(corr);
         if (lane == 0 && g + corr >= 0) {
             flags[v] = 1;
             const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
             movers[slot] = v;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree),
+                      static_cast<unsigned long long>(static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v])));
         }
     }
 }
@@ -175,22 +215,29 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
 }
 
 // incremental_commit (src/refine_incremental.cuh:97-109); also clears the
-// mover flag so that `flags` is all-zero outside an apply.
+// mover flag so that `flags` is all-zero outside an apply.  Part-weight
+// changes are summed per block in shared memory first: all movers hit the
+// same k counters, so global atomics would serialise.
 template <typename W>
 __global__ void commit_kernel(const i32* __restrict__ movers, const RefineCounters* ctr_in,
                               i32* labels, const i32* __restrict__ targets, const W* __restrict__ vw, u64* pw,
                               unsigned char* locks, unsigned char* flags, int lp) {
+    __shared__ unsigned long long delta[32];
+    if (threadIdx.x < 32) delta[threadIdx.x] = 0;
+    __syncthreads();
     const i64 count = ctr_in->movers;
     for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += static_cast<i64>(gridDim.x) * blockDim.x) {
         const i32 v = movers[i];
         const i32 s = labels[v], t = targets[v];
         const u64 w = static_cast<u64>(weight_at(vw, v));
-        atomic_add_u64(&pw[s], 0ULL - w);
-        atomic_add_u64(&pw[t], w);
+        atomicAdd(&delta[s], 0ULL - w);
+        atomicAdd(&delta[t], static_cast<unsigned long long>(w));
         labels[v] = t;
         if (lp) locks[v] = 1;
         flags[v] = 0;
     }
+    __syncthreads();
+    if (threadIdx.x < 32 && delta[threadIdx.x]) atomic_add_u64(&pw[threadIdx.x], delta[threadIdx.x]);
 }
 
 // Rebalance gain bucket (refine_incremental.cuh:167-171) restated with host

@@ -35,6 +35,7 @@ struct RoundParams {
     int filter;      // role filtering (rounds 0-3); off for the two-hop pass
     int identity;    // clusters are the identity (round 0): skip the gather
     int two_hop;     // write favourites instead of LP proposals
+    int sum32;       // every connection sum fits 32 bits (total edge weight < 2^32)
 };
 
 // Salts of src/coarsen.cu:1152-1157.
@@ -46,6 +47,7 @@ inline RoundParams make_round(u32 seed, int level, int round, bool filter, u32 m
     p.filter = filter ? 1 : 0;
     p.identity = round == 0 ? 1 : 0;
     p.two_hop = 0;
+    p.sum32 = 0;
     return p;
 }
 
@@ -136,11 +138,15 @@ __global__ void __launch_bounds__(kThreads) affinity_small_kernel(
     }
     const unsigned peers = __match_any_sync(mask, valid ? c : -1);
     u64 conn = 0;
-    const int base = lane & ~(G - 1);
+    if (p.sum32) {
+        conn = __reduce_add_sync(peers, static_cast<u32>(w));
+    } else {
+        const int base = lane & ~(G - 1);
 #pragma unroll
-    for (int s = 0; s < G; ++s) {
-        const u64 pw = __shfl_sync(mask, w, base + s);
-        if (peers & (1u << (base + s))) conn += pw;
+        for (int s = 0; s < G; ++s) {
+            const u64 pw = __shfl_sync(mask, w, base + s);
+            if (peers & (1u << (base + s))) conn += pw;
+        }
     }
     const bool leader = valid && lane == __ffs(peers) - 1;
     const i32 source = has_vertex ? (p.identity ? v : clusters[v]) : -1;
