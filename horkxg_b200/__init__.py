@@ -59,7 +59,8 @@ class RefineStats(ctypes.Structure):
 EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_error", "gp_partition_capacity",
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
-           "gp_launch_count", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump"]
+           "gp_launch_count", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
+           "gp_initial_partition_static"]
 
 _LIB = None
 
@@ -96,6 +97,8 @@ def lib() -> ctypes.CDLL:
         L.gp_ctx_stream.restype = vp
         L.gp_profile_enable.argtypes = [vp, i32]
         L.gp_profile_dump.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64]
+        L.gp_initial_partition_static.argtypes = [P(GraphDesc), i32, dbl, u32, vp, vp, ctypes.c_char_p,
+                                                  ctypes.c_uint64]
         _LIB = L
     return _LIB
 

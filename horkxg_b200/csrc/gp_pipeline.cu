@@ -14,6 +14,7 @@
 #include <iostream>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <string>
@@ -1373,6 +1374,175 @@ void host_level_copy(Device& d, const DGraph<T>& g, const i32* map, i64 map_n, s
     for (i64 i = 0; i < g.n; ++i) vw[i] = g.vwp() ? static_cast<u64>(v[i]) : 1;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free spectral initial partition.
+//
+// Some callers cannot allocate device memory: a process whose device memory
+// is owned by another allocator (a framework's pool that accounts for every
+// byte, where a raw cudaMalloc bypasses its budget and can fail or fragment
+// it), and latency-bound callers for which cudaMalloc's implicit
+// synchronisation and unpredictable cost are not acceptable.  For small
+// graphs -- the coarsest level of a hierarchy, at most kStaticMaxVertices
+// vertices -- the recursive bisection runs entirely in a fixed scratch array
+// that every GPU loading this library holds until exit.  The kernels are the
+// ones of initial_partition(); only the memory comes from the array.
+// ---------------------------------------------------------------------------
+constexpr i64 kStaticMaxVertices = 65536;
+constexpr size_t kStaticScratchBytes = size_t{4} << 20;   // 4 MiB
+constexpr int kStaticMaxDepths = 6;
+constexpr int kStaticMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+struct StaticScratch {
+    u32* err;
+    u32* bar;
+    u64* stats;
+    u64* loads;
+    InitTask* tasks;   // kStaticMaxDepths x kMaxInitTasks
+    i32* order;
+    i32* task_of_pos;
+    float* deg;
+    float* xa;
+    float* xb;
+    Moments* contrib;
+    u64* key;
+    u64* key_alt;
+    u64* prefix;
+};
+
+inline StaticScratch carve_static(unsigned char* base) {
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + at;
+        at += (bytes + 255) & ~size_t{255};
+        return p;
+    };
+    const size_t n = static_cast<size_t>(kStaticMaxVertices);
+    StaticScratch s;
+    s.err = reinterpret_cast<u32*>(take(sizeof(u32)));
+    s.bar = reinterpret_cast<u32*>(take(2 * sizeof(u32)));
+    s.stats = reinterpret_cast<u64*>(take(8 * sizeof(u64)));
+    s.loads = reinterpret_cast<u64*>(take(33 * sizeof(u64)));
+    s.tasks = reinterpret_cast<InitTask*>(take(kStaticMaxDepths * kMaxInitTasks * sizeof(InitTask)));
+    s.order = reinterpret_cast<i32*>(take(n * sizeof(i32)));
+    s.task_of_pos = reinterpret_cast<i32*>(take(n * sizeof(i32)));
+    s.deg = reinterpret_cast<float*>(take(n * sizeof(float)));
+    s.xa = reinterpret_cast<float*>(take(n * sizeof(float)));
+    s.xb = reinterpret_cast<float*>(take(n * sizeof(float)));
+    s.contrib = reinterpret_cast<Moments*>(take(n * sizeof(Moments)));
+    s.key = reinterpret_cast<u64*>(take(n * sizeof(u64)));
+    s.key_alt = reinterpret_cast<u64*>(take(n * sizeof(u64)));
+    s.prefix = reinterpret_cast<u64*>(take(n * sizeof(u64)));
+    if (at > kStaticScratchBytes) fail(GP_ERUNTIME, "static scratch layout exceeds its array");
+    return s;
+}
+
+// Device address of the scratch array on the current device, looked up once
+// per device with cudaGetSymbolAddress (a host-side reference to the array
+// is not a device address).
+inline unsigned char* static_scratch_address() {
+    static std::mutex mutex;
+    static unsigned char* address[kStaticMaxDevices] = {};
+    int dev = 0;
+    GP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices) fail(GP_EINVAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!address[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) fail(GP_ECUDA, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+        address[dev] = static_cast<unsigned char*>(p);
+    }
+    return address[dev];
+}
+
+template <typename T>
+void initial_partition_static(const gp_graph* gi, int parts, double ratio, u32 seed, i32* labels,
+                              cudaStream_t stream) {
+    using O = typename T::O;
+    using W = typename T::W;
+    if (!gi || gi->memory != GP_MEMORY_DEVICE || gi->index64)
+        fail(GP_EINVAL, "the graph must be in device memory in the width's own types");
+    if (!labels) fail(GP_EINVAL, "labels must be a device array of n entries");
+    const i64 n64 = gi->n;
+    if (n64 > kStaticMaxVertices)
+        fail(GP_EINVAL, "graph has " + std::to_string(n64) + " vertices; the allocation-free initial partition "
+                        "supports at most " + std::to_string(kStaticMaxVertices));
+    if (n64 <= 0 || parts < 2 || parts > n64 || parts > 32 || !std::isfinite(ratio) || ratio < 1.0)
+        fail(GP_EINVAL, "invalid GPU initial partition input");
+    const i32 n = static_cast<i32>(n64);
+    const StaticScratch sc = carve_static(static_scratch_address());
+
+    // A Device without an allocator: launches, stream and error word only.
+    Device d;
+    GP_CUDA(cudaGetDevice(&d.device));
+    GP_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, d.device));
+    d.stream = stream;
+    d.err = sc.err;
+    auto read = [&](void* host, const void* dev, size_t bytes) {
+        GP_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, stream));
+        GP_CUDA(cudaStreamSynchronize(stream));
+    };
+    // The array keeps the previous call's contents: clear what starts at zero.
+    GP_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(u32), stream));
+    GP_CUDA(cudaMemsetAsync(sc.stats, 0, 8 * sizeof(u64), stream));
+    GP_CUDA(cudaMemsetAsync(sc.loads, 0, 33 * sizeof(u64), stream));
+    GP_CUDA(cudaMemsetAsync(labels, 0, static_cast<size_t>(n) * sizeof(i32), stream));
+
+    DGraph<T> g;   // borrowed views of the caller's arrays
+    g.n = n64;
+    g.m = gi->m;
+    g.off.borrow(static_cast<O*>(const_cast<void*>(gi->offsets)), static_cast<size_t>(n) + 1);
+    g.nbr.borrow(static_cast<i32*>(const_cast<void*>(gi->neighbors)), static_cast<size_t>(gi->m));
+    g.unit_ew = gi->edge_weights == nullptr;
+    g.unit_vw = gi->vertex_weights == nullptr;
+    if (!g.unit_ew) g.ew.borrow(static_cast<W*>(const_cast<void*>(gi->edge_weights)), static_cast<size_t>(gi->m));
+    if (!g.unit_vw) g.vw.borrow(static_cast<W*>(const_cast<void*>(gi->vertex_weights)), static_cast<size_t>(n));
+
+    launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, n), kThreads, 0, n, g.vwp(), sc.stats);
+    launch(d, "sat_sum_kernel", sat_sum_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), sc.stats + 2);
+    u64 st[3];
+    read(st, sc.stats, sizeof(st));
+    const u64 total = st[0], maxw = st[1], edge_total = st[2];
+    if (!total || total == ~0ULL || edge_total == ~0ULL)
+        fail(GP_EOVERFLOW, "GPU initializer weight accumulation overflow");
+    const u64 capacity = partition_capacity(total, parts, ratio);
+    if (maxw > capacity) fail(GP_EINVAL, "a vertex exceeds partition capacity");
+
+    auto depths = plan_tasks(parts);
+    if (static_cast<int>(depths.size()) > kStaticMaxDepths) fail(GP_ERUNTIME, "task tree deeper than expected");
+    depths[0].tasks[0].count = n;
+    depths[0].tasks[0].weight = total;
+    for (size_t dpt = 0; dpt < depths.size(); ++dpt)
+        GP_CUDA(cudaMemcpyAsync(sc.tasks + dpt * kMaxInitTasks, depths[dpt].tasks.data(),
+                                depths[dpt].tasks.size() * sizeof(InitTask), cudaMemcpyHostToDevice, stream));
+    launch(d, "iota_kernel", iota_kernel, blocks_for(n, kThreads), kThreads, 0, n, sc.order);
+    for (size_t dpt = 0; dpt < depths.size(); ++dpt) {
+        const int nt = static_cast<int>(depths[dpt].tasks.size());
+        InitTask* tasks = sc.tasks + dpt * kMaxInitTasks;
+        GP_CUDA(cudaMemsetAsync(sc.task_of_pos, 0xff, static_cast<size_t>(n) * sizeof(i32), stream));
+        launch(d, "task_positions_kernel", task_positions_kernel, nt, kThreads, 0, nt, tasks, sc.task_of_pos);
+        launch_diffusion(d, g, nt, tasks, sc.task_of_pos, n, sc.order, labels, seed, 64, sc.deg, sc.xa, sc.xb,
+                         sc.contrib, nullptr, sc.key, sc.bar);
+        launch(d, "task_sort_kernel", task_sort_kernel, nt, kThreads, 0, nt, tasks, sc.key, sc.key_alt, sc.order);
+        InitTask* next = dpt + 1 < depths.size() ? sc.tasks + (dpt + 1) * kMaxInitTasks : nullptr;
+        launch(d, "task_split_kernel", task_split_kernel<W>, nt, kThreads, 0, nt, tasks, next, sc.order, g.vwp(),
+               capacity, sc.prefix, labels, sc.err);
+    }
+    launch(d, "part_weight_kernel", part_weight_kernel<W>, blocks_for(n, kThreads), kThreads, 0, n, labels, g.vwp(),
+           sc.loads);
+    u32 e = 0;
+    read(&e, sc.err, sizeof(e));
+    if (e & kErrTimeout) fail(GP_ETIMEOUT, "a bounded device wait timed out");
+    if (e & kErrSplit) fail(GP_ERUNTIME, "GPU spectral split cannot satisfy capacity");
+    if (e & kErrBalance) fail(GP_ERUNTIME, "GPU initializer infeasible balance");
+    if (e) fail(GP_ERUNTIME, "device error during the initial partition");
+    u64 loads[32];
+    read(loads, sc.loads, static_cast<size_t>(parts) * sizeof(u64));
+    if (*std::max_element(loads, loads + parts) > capacity) fail(GP_ERUNTIME, "GPU initializer balance validation failed");
+}
+
 }  // namespace gp
 
 // ---------------------------------------------------------------------------
@@ -1800,6 +1970,30 @@ gp_status gp_refine(gp_ctx* ctx, const gp_graph* graph, int32_t* labels, int par
 }
 
 uint64_t gp_launch_count(const gp_ctx* ctx) { return ctx ? ctx->dev.launches : 0; }
+
+gp_status gp_initial_partition_static(const gp_graph* graph, int parts, double ratio, uint32_t seed, int32_t* labels,
+                                      void* stream, char* message, uint64_t message_capacity) {
+    std::string what;
+    gp_status status = GP_OK;
+    try {
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            gp::initial_partition_static<T>(graph, parts, ratio, seed, labels, static_cast<cudaStream_t>(stream));
+        });
+    } catch (const gp::Error& e) {
+        status = e.status;
+        what = e.what();
+    } catch (const std::exception& e) {
+        status = GP_ERUNTIME;
+        what = e.what();
+    }
+    if (message && message_capacity) {
+        const size_t k = std::min<size_t>(what.size(), static_cast<size_t>(message_capacity) - 1);
+        std::memcpy(message, what.data(), k);
+        message[k] = 0;
+    }
+    return status;
+}
 
 void* gp_ctx_stream(const gp_ctx* ctx) { return ctx ? static_cast<void*>(ctx->dev.stream) : nullptr; }
 

@@ -181,6 +181,30 @@ gp_status gp_cut(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int 
  * library's own sm_100a kernels). */
 uint64_t gp_launch_count(const gp_ctx* ctx);
 
+/* Spectral initial partition that allocates no device memory.
+ *
+ * For callers that cannot call cudaMalloc: a process whose device memory is
+ * owned by another allocator (a framework pool that accounts for every byte;
+ * a raw cudaMalloc would bypass its budget and can fail or fragment it), or a
+ * latency-bound caller that cannot afford cudaMalloc's implicit
+ * synchronisation.  This entry point has no counterpart in the reference;
+ * it computes the same labels as gp_initial_partition.
+ *
+ * The caller passes the graph in device memory in the width's own types
+ * (index64 = 0; at most 65536 vertices -- larger graphs are rejected with
+ * GP_EINVAL), `labels` as a device array of n int32 entries, and the stream
+ * to run on (NULL = the legacy default stream).  All scratch lives in a 4 MiB
+ * array compiled into the library, which every GPU that loads the library
+ * holds until the process exits.  The first call on a device looks the
+ * array's device address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Every call shares the one array, so calls that
+ * overlap on the GPU (concurrent streams or threads) race and must be
+ * serialised by the caller.  On failure a message is written to `message`
+ * (if not NULL, at most message_capacity bytes including the terminator). */
+gp_status gp_initial_partition_static(const gp_graph* graph, int parts, double ratio, uint32_t seed,
+                                      int32_t* labels, void* stream, char* message,
+                                      uint64_t message_capacity);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events with the library's. */
 void* gp_ctx_stream(const gp_ctx* ctx);
