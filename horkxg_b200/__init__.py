@@ -49,6 +49,12 @@ class Report(ctypes.Structure):
                 ("prepare_seconds", ctypes.c_double)]
 
 
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("slot", ctypes.c_int32), ("queued_seconds", ctypes.c_double),
+                ("service_seconds", ctypes.c_double), ("latency_seconds", ctypes.c_double),
+                ("footprint_bytes", ctypes.c_uint64), ("message", ctypes.c_char * 192)]
+
+
 class RefineStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_int32), ("proposals", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
                 ("initial_cut", ctypes.c_uint64), ("final_cut", ctypes.c_uint64),
@@ -60,7 +66,9 @@ EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_erro
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
            "gp_launch_count", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
-           "gp_initial_partition_static"]
+           "gp_initial_partition_static", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
+           "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
+           "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
 
 _LIB = None
 
@@ -99,6 +107,21 @@ def lib() -> ctypes.CDLL:
         L.gp_profile_dump.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64]
         L.gp_initial_partition_static.argtypes = [P(GraphDesc), i32, dbl, u32, vp, vp, ctypes.c_char_p,
                                                   ctypes.c_uint64]
+        u64 = ctypes.c_uint64
+        L.gp_partition_range.argtypes = [vp, P(GraphDesc), i64, i64, P(Options), vp, P(Report)]
+        L.gp_ctx_memory.argtypes = [vp, P(u64), P(u64), P(u64), i32]
+        L.gp_ctx_trim.argtypes = [vp]
+        L.gp_footprint_bytes.argtypes = [i64, i64, i32, i32, i32]
+        L.gp_footprint_bytes.restype = u64
+        L.gp_server_create.argtypes = [i32, i32, u64, P(vp)]
+        L.gp_server_destroy.argtypes = [vp]
+        L.gp_server_error.argtypes = [vp]
+        L.gp_server_error.restype = ctypes.c_char_p
+        L.gp_server_submit.argtypes = [vp, P(GraphDesc), P(Options), vp, P(u64)]
+        L.gp_server_submit_range.argtypes = [vp, P(GraphDesc), i64, i64, P(Options), vp, P(u64)]
+        L.gp_server_poll.argtypes = [vp, u64, P(i32)]
+        L.gp_server_wait.argtypes = [vp, u64, P(Report), P(RequestInfo)]
+        L.gp_partition_batch.argtypes = [vp, P(GraphDesc), i32, vp, vp, vp, vp, vp]
         _LIB = L
     return _LIB
 
@@ -152,6 +175,132 @@ class HostGraph:
         d.edge_weights = None if self.ew is None else self.ew.ctypes.data
         d.vertex_weights = None if self.vw is None else self.vw.ctypes.data
         return d
+
+
+class PackedGraph:
+    """Several graphs in one concatenated CSR: global int64 offsets into the
+    concatenated neighbour array, neighbour ids local to their instance, and
+    per-instance vertex offsets (the layout gp_partition_range and
+    gp_partition_batch take)."""
+
+    def __init__(self, offsets, neighbors, vertex_offsets, width: int = STANDARD):
+        self.width = width
+        self.off = np.ascontiguousarray(offsets, dtype=np.int64)
+        self.nbr = np.ascontiguousarray(neighbors, dtype=np.int32)
+        self.vertex_offsets = np.ascontiguousarray(vertex_offsets, dtype=np.int64)
+        self.n = len(self.off) - 1
+        self.m = len(self.nbr)
+        self.count = len(self.vertex_offsets) - 1
+
+    @classmethod
+    def pack(cls, graphs, width: int = STANDARD) -> "PackedGraph":
+        """graphs: iterable of (offsets, neighbours) pairs with local ids."""
+        graphs = list(graphs)
+        vo = np.zeros(len(graphs) + 1, np.int64)
+        for i, (off, _) in enumerate(graphs):
+            vo[i + 1] = vo[i] + len(off) - 1
+        off_all = np.zeros(int(vo[-1]) + 1, np.int64)
+        nbr_all = np.concatenate([np.asarray(nb, np.int32) for _, nb in graphs]) if graphs else np.zeros(0, np.int32)
+        base = 0
+        for i, (off, nb) in enumerate(graphs):
+            off = np.asarray(off, np.int64)
+            off_all[vo[i]:vo[i + 1] + 1] = off + base
+            base += len(nb)
+        return cls(off_all, nbr_all, vo, width)
+
+    def instance(self, i: int):
+        a, b = int(self.vertex_offsets[i]), int(self.vertex_offsets[i + 1])
+        e0, e1 = int(self.off[a]), int(self.off[b])
+        return self.off[a:b + 1] - e0, self.nbr[e0:e1]
+
+    def desc(self) -> GraphDesc:
+        # int64 offsets with int32 neighbours (index64 = 2)
+        d = GraphDesc()
+        d.n, d.m, d.width, d.memory, d.index64 = self.n, self.m, self.width, HOST, 2
+        d.offsets = self.off.ctypes.data
+        d.neighbors = self.nbr.ctypes.data
+        return d
+
+
+def footprint_bytes(n: int, m: int, parts: int, width: int = STANDARD, index64_host: bool = False) -> int:
+    return int(lib().gp_footprint_bytes(n, m, parts, width, int(index64_host)))
+
+
+class Server:
+    """Continuous-batching partition server on one GPU (gp_server_*): `slots`
+    contexts with their own streams, FIFO admission under a device memory
+    budget."""
+
+    def __init__(self, device: int = 0, slots: int = 8, memory_budget: int = 120 << 30):
+        self._h = ctypes.c_void_p()
+        rc = lib().gp_server_create(device, slots, memory_budget, ctypes.byref(self._h))
+        if rc:
+            raise PartitionError(rc, "cannot create server")
+        self._live = {}
+
+    def close(self):
+        if self._h:
+            lib().gp_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, g: HostGraph, options: Options | None = None, **kw) -> int:
+        o = options or default_options(**kw)
+        labels = np.zeros(g.n, np.int32)
+        d = g.desc()
+        t = ctypes.c_uint64()
+        rc = lib().gp_server_submit(self._h, ctypes.byref(d), ctypes.byref(o), labels.ctypes.data, ctypes.byref(t))
+        if rc:
+            raise PartitionError(rc, lib().gp_server_error(self._h).decode())
+        self._live[t.value] = (g, d, o, labels)
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        done = ctypes.c_int32()
+        rc = lib().gp_server_poll(self._h, ticket, ctypes.byref(done))
+        if rc:
+            raise PartitionError(rc, "unknown ticket")
+        return bool(done.value)
+
+    def wait(self, ticket: int):
+        """Returns (labels, report, info); raises on a failed request."""
+        rep, info = Report(), RequestInfo()
+        rc = lib().gp_server_wait(self._h, ticket, ctypes.byref(rep), ctypes.byref(info))
+        g, d, o, labels = self._live.pop(ticket, (None, None, None, None))
+        if rc:
+            raise PartitionError(rc, info.message.decode() or "unknown ticket")
+        return labels, rep, info
+
+    def partition_batch(self, packed: PackedGraph, options=None):
+        """Partition every instance of a packed CSR; options: one Options or a
+        list of them.  Returns (labels of all instances, list of reports)."""
+        count = packed.count
+        if options is None:
+            options = default_options()
+        if isinstance(options, Options):
+            options = [options] * count
+        opts = (Options * max(count, 1))(*options)
+        reps = (Report * max(count, 1))()
+        st = np.zeros(max(count, 1), np.int32)
+        labels = np.zeros(packed.n, np.int32)
+        d = packed.desc()
+        rc = lib().gp_partition_batch(self._h, ctypes.byref(d), count, packed.vertex_offsets.ctypes.data, opts,
+                                      labels.ctypes.data, reps, st.ctypes.data)
+        if rc:
+            raise PartitionError(rc, lib().gp_server_error(self._h).decode())
+        return labels, [reps[i] for i in range(count)]
 
 
 class Context:
@@ -220,6 +369,26 @@ class Context:
         self._check(lib().gp_partition(self._h, ctypes.byref(d), ctypes.byref(o), labels.ctypes.data,
                                        ctypes.byref(rep)))
         return labels, rep
+
+    def partition_range(self, packed: PackedGraph, i: int, options: Options | None = None, **kw):
+        """Partition instance i of a packed CSR, as gp_partition would alone."""
+        o = options or default_options(**kw)
+        a, b = int(packed.vertex_offsets[i]), int(packed.vertex_offsets[i + 1])
+        labels = np.zeros(b - a, np.int32)
+        rep = Report()
+        d = packed.desc()
+        self._check(lib().gp_partition_range(self._h, ctypes.byref(d), a, b, ctypes.byref(o), labels.ctypes.data,
+                                             ctypes.byref(rep)))
+        return labels, rep
+
+    def memory(self, reset_peak: bool = False) -> dict:
+        live, cached, peak = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().gp_ctx_memory(self._h, ctypes.byref(live), ctypes.byref(cached), ctypes.byref(peak),
+                                        int(reset_peak)))
+        return {"live": live.value, "cached": cached.value, "peak": peak.value}
+
+    def trim(self):
+        self._check(lib().gp_ctx_trim(self._h))
 
     def aggregate(self, g: HostGraph, parts: int, seed: int, level: int, cluster_size_factor: int = 256,
                   pack_isolated: bool = False):

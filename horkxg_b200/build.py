@@ -39,8 +39,9 @@ def _stale(target: Path, sources: list[Path]) -> bool:
 def build(force: bool = False) -> None:
     headers = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "gpart_b200.h"]
     lib = PKG / "libgpart_b200.so"
-    if force or _stale(lib, [CSRC / "gp_pipeline.cu", *headers]):
-        _run([NVCC, *NVFLAGS, "-shared", "-o", str(lib), str(CSRC / "gp_pipeline.cu")])
+    sources = [CSRC / "gp_pipeline.cu", CSRC / "gp_serve.cpp"]
+    if force or _stale(lib, [*sources, *headers]):
+        _run([NVCC, *NVFLAGS, "-shared", "-I", str(ROOT / "include"), "-o", str(lib), *map(str, sources)])
     bindir = PKG / "bin"
     bindir.mkdir(exist_ok=True)
     for width, macro in (("standard", "GP_WIDTH_STANDARD"), ("big", "GP_WIDTH_BIG")):

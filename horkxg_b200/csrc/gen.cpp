@@ -114,12 +114,15 @@ void pairs_to_csr(i64 n, const std::vector<u32>& src, const std::vector<u32>& ds
     });
 }
 
-void emit(const std::vector<i64>& offsets, const std::vector<i64>& indices,
-          const char* indptr_path, const char* indices_path, i64* n_out, i64* m_out) {
-    write_file(indptr_path, offsets.data(), offsets.size() * sizeof(i64));
-    write_file(indices_path, indices.data(), indices.size() * sizeof(i64));
-    *n_out = static_cast<i64>(offsets.size()) - 1;
-    *m_out = static_cast<i64>(indices.size());
+struct Csr {
+    std::vector<i64> off, idx;
+};
+
+void emit(const Csr& g, const char* indptr_path, const char* indices_path, i64* n_out, i64* m_out) {
+    write_file(indptr_path, g.off.data(), g.off.size() * sizeof(i64));
+    write_file(indices_path, g.idx.data(), g.idx.size() * sizeof(i64));
+    *n_out = static_cast<i64>(g.off.size()) - 1;
+    *m_out = static_cast<i64>(g.idx.size());
 }
 
 template <typename F>
@@ -127,15 +130,23 @@ int guarded(F&& f) {
     try { f(); return 0; } catch (const std::exception& e) { g_error = e.what(); return 1; }
 }
 
-}  // namespace
+template <typename F>
+void* hold(F&& build, i64* n, i64* m) {
+    try {
+        auto* g = new Csr(build());
+        *n = static_cast<i64>(g->off.size()) - 1;
+        *m = static_cast<i64>(g->idx.size());
+        return g;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return nullptr;
+    }
+}
 
-extern "C" {
-
-const char* gp_gen_last_error(void) { return g_error.c_str(); }
 
 // 2D 5-point grid, vertex id = row * nx + column.
-int gp_gen_grid2d(i64 nx, i64 ny, const char* indptr_path, const char* indices_path, i64* n, i64* m) {
-    return guarded([&] {
+Csr build_grid2d(i64 nx, i64 ny) {
+    {
         if (nx < 1 || ny < 1) throw std::runtime_error("invalid grid");
         const i64 nv = nx * ny;
         std::vector<i64> off(static_cast<size_t>(nv) + 1, 0), idx;
@@ -154,13 +165,13 @@ int gp_gen_grid2d(i64 nx, i64 ny, const char* indptr_path, const char* indices_p
                 if (y + 1 < ny) idx[p++] = v + nx;
             }
         });
-        emit(off, idx, indptr_path, indices_path, n, m);
-    });
+        return Csr{std::move(off), std::move(idx)};
+    }
 }
 
 // 3D 7-point grid, vertex id = (z * ny + y) * nx + x.
-int gp_gen_grid3d(i64 nx, i64 ny, i64 nz, const char* indptr_path, const char* indices_path, i64* n, i64* m) {
-    return guarded([&] {
+Csr build_grid3d(i64 nx, i64 ny, i64 nz) {
+    {
         if (nx < 1 || ny < 1 || nz < 1) throw std::runtime_error("invalid grid");
         const i64 plane = nx * ny, nv = plane * nz;
         std::vector<i64> off(static_cast<size_t>(nv) + 1, 0), idx;
@@ -181,17 +192,16 @@ int gp_gen_grid3d(i64 nx, i64 ny, i64 nz, const char* indptr_path, const char* i
                 if (z + 1 < nz) idx[p++] = v + plane;
             }
         });
-        emit(off, idx, indptr_path, indices_path, n, m);
-    });
+        return Csr{std::move(off), std::move(idx)};
+    }
 }
 
 // R-MAT with 2^scale vertices and edge_factor * 2^scale generated pairs,
 // quadrant probabilities (a, b, c, 1-a-b-c); vertex ids are relabelled by a
 // seeded random permutation; pairs are symmetrised with self loops and
 // duplicates removed.
-int gp_gen_rmat(int scale, int edge_factor, double a, double b, double c, u64 seed,
-                const char* indptr_path, const char* indices_path, i64* n, i64* m) {
-    return guarded([&] {
+Csr build_rmat(int scale, int edge_factor, double a, double b, double c, u64 seed) {
+    {
         if (scale < 1 || scale > 30 || edge_factor < 1) throw std::runtime_error("invalid rmat");
         const i64 nv = i64{1} << scale;
         const i64 pairs = nv * edge_factor;
@@ -225,17 +235,16 @@ int gp_gen_rmat(int scale, int edge_factor, double a, double b, double c, u64 se
         });
         std::vector<i64> off, idx;
         pairs_to_csr(nv, src, dst, off, idx);
-        emit(off, idx, indptr_path, indices_path, n, m);
-    });
+        return Csr{std::move(off), std::move(idx)};
+    }
 }
 
 // Random geometric graph: nv points uniform in the unit square, an edge for
 // every pair at Euclidean distance < radius.  Vertices are numbered in
 // row-major cell order (cells of side >= radius), which keeps neighbours
 // close in id space as spatial generators usually do.
-int gp_gen_rgg(i64 nv, double radius, u64 seed, const char* indptr_path, const char* indices_path,
-               i64* n, i64* m) {
-    return guarded([&] {
+Csr build_rgg(i64 nv, double radius, u64 seed) {
+    {
         if (nv < 1 || !(radius > 0)) throw std::runtime_error("invalid rgg");
         const u64 stream = splitmix64(seed * 0x9e3779b97f4a7c15ULL + 0x2545f4914f6cdd1dULL);
         std::vector<double> px(static_cast<size_t>(nv)), py(static_cast<size_t>(nv));
@@ -288,8 +297,66 @@ int gp_gen_rgg(i64 nv, double radius, u64 seed, const char* indptr_path, const c
         parallel_for(nv, [&](i64 lo, i64 hi) {
             for (i64 v = lo; v < hi; ++v) std::copy(rows[v].begin(), rows[v].end(), idx.begin() + off[v]);
         });
-        emit(off, idx, indptr_path, indices_path, n, m);
+        return Csr{std::move(off), std::move(idx)};
+    }
+}
+
+
+}  // namespace
+
+extern "C" {
+
+const char* gp_gen_last_error(void) { return g_error.c_str(); }
+
+int gp_gen_grid2d(i64 nx, i64 ny, const char* indptr_path, const char* indices_path, i64* n, i64* m) {
+    return guarded([&] { emit(build_grid2d(nx, ny), indptr_path, indices_path, n, m); });
+}
+
+int gp_gen_grid3d(i64 nx, i64 ny, i64 nz, const char* indptr_path, const char* indices_path, i64* n, i64* m) {
+    return guarded([&] { emit(build_grid3d(nx, ny, nz), indptr_path, indices_path, n, m); });
+}
+
+int gp_gen_rmat(int scale, int edge_factor, double a, double b, double c, u64 seed,
+                const char* indptr_path, const char* indices_path, i64* n, i64* m) {
+    return guarded([&] { emit(build_rmat(scale, edge_factor, a, b, c, seed), indptr_path, indices_path, n, m); });
+}
+
+int gp_gen_rgg(i64 nv, double radius, u64 seed, const char* indptr_path, const char* indices_path,
+               i64* n, i64* m) {
+    return guarded([&] { emit(build_rgg(nv, radius, seed), indptr_path, indices_path, n, m); });
+}
+
+// In-memory variants: the graph is kept in a handle; gp_gen_copy writes its
+// offsets (int64) and neighbours (int32 or int64) into caller arrays.
+void* gp_gen_grid2d_new(i64 nx, i64 ny, i64* n, i64* m) {
+    return hold([&] { return build_grid2d(nx, ny); }, n, m);
+}
+
+void* gp_gen_rmat_new(int scale, int edge_factor, double a, double b, double c, u64 seed, i64* n, i64* m) {
+    return hold([&] { return build_rmat(scale, edge_factor, a, b, c, seed); }, n, m);
+}
+
+void* gp_gen_rgg_new(i64 nv, double radius, u64 seed, i64* n, i64* m) {
+    return hold([&] { return build_rgg(nv, radius, seed); }, n, m);
+}
+
+int gp_gen_copy(const void* handle, i64* offsets, void* neighbors, int neighbor_bytes) {
+    return guarded([&] {
+        const auto* g = static_cast<const Csr*>(handle);
+        if (!g || (neighbor_bytes != 4 && neighbor_bytes != 8)) throw std::runtime_error("invalid copy");
+        if (offsets) std::copy(g->off.begin(), g->off.end(), offsets);
+        if (!neighbors) return;
+        if (neighbor_bytes == 8) {
+            std::copy(g->idx.begin(), g->idx.end(), static_cast<i64*>(neighbors));
+        } else {
+            auto* out = static_cast<std::int32_t*>(neighbors);
+            parallel_for(static_cast<i64>(g->idx.size()), [&](i64 lo, i64 hi) {
+                for (i64 i = lo; i < hi; ++i) out[i] = static_cast<std::int32_t>(g->idx[i]);
+            });
+        }
     });
 }
+
+void gp_gen_free(void* handle) { delete static_cast<Csr*>(handle); }
 
 }  // extern "C"

@@ -87,7 +87,7 @@ struct Device {
 
     std::map<size_t, std::vector<void*>> free_blocks;
     std::unordered_map<void*, size_t> live;
-    size_t cached_bytes = 0, live_bytes = 0;
+    size_t cached_bytes = 0, live_bytes = 0, peak_bytes = 0;
     u64 alloc_calls = 0, driver_allocs = 0;
     double alloc_ms = 0.0;   // host time spent inside the allocator
 
@@ -131,6 +131,7 @@ struct Device {
         }
         live[p] = c;
         live_bytes += c;
+        peak_bytes = std::max(peak_bytes, live_bytes);
         ++alloc_calls;
         alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return p;

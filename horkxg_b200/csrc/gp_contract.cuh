@@ -247,9 +247,11 @@ __global__ void __launch_bounds__(kThreads) segment_global_kernel(i64 rows, cons
 }
 
 // Row-size classes: 0 empty, 1 <= 32, 2 <= smem_cap, 3 larger.
-__global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u64* keys, i32* vals, u32* counts) {
-    __shared__ u32 local[4];
-    if (threadIdx.x < 4) local[threadIdx.x] = 0;
+// Classifies coarse rows by their number of scattered entries.  counts[0..3]
+// receive the rows per class, counts[4..7] the entries per class.
+__global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u64* keys, i32* vals, u64* counts) {
+    __shared__ unsigned long long local[8];
+    if (threadIdx.x < 8) local[threadIdx.x] = 0;
     __syncthreads();
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c < rows) {
@@ -257,10 +259,12 @@ __global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u6
         const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= smem_cap ? 2 : 3;
         keys[c] = static_cast<u64>(k);
         vals[c] = static_cast<i32>(c);
-        atomicAdd(&local[k], 1u);
+        atomicAdd(&local[k], 1ull);
+        atomicAdd(&local[4 + k], static_cast<unsigned long long>(l));
     }
     __syncthreads();
-    if (threadIdx.x < 4 && local[threadIdx.x]) atomicAdd(&counts[threadIdx.x], local[threadIdx.x]);
+    if (threadIdx.x < 8 && local[threadIdx.x])
+        atomicAdd(reinterpret_cast<unsigned long long*>(&counts[threadIdx.x]), local[threadIdx.x]);
 }
 
 template <typename O>

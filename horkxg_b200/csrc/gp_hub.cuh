@@ -125,10 +125,11 @@ constexpr i64 kSlotTile = 2048;
 template <typename W>
 __global__ void __launch_bounds__(kThreads) hub_candidates_kernel(
     i64 hubs, const i32* __restrict__ hub_list, const i64* __restrict__ table_off, HubSlot* table,
-    const i32* __restrict__ clusters, RoundParams p, HubPartial* partials) {
+    const i32* __restrict__ clusters, RoundParams p, HubPartial* partials, i64 tile_base) {
     __shared__ CandShared red;
     __shared__ int hub_sh;
-    const i64 s0 = static_cast<i64>(blockIdx.x) * kSlotTile;
+    const i64 tile = tile_base + blockIdx.x;  // tile_base offsets a launch over a sub-range of tables
+    const i64 s0 = tile * kSlotTile;
     if (threadIdx.x == 0) {
         i64 lo = 0, hi = hubs - 1;   // last hub with table_off <= s0
         while (lo < hi) {
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) hub_candidates_kernel(
         }
     }
     block_candidate_reduce(current, best, tie, red);
-    if (threadIdx.x == 0) partials[blockIdx.x] = {current, best, tie};
+    if (threadIdx.x == 0) partials[tile] = {current, best, tie};
 }
 
 template <typename W>

@@ -313,6 +313,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     // hash-free affinity on identity rounds (rows without duplicates)
     const bool direct_ok = unique_rows(d, g);
     // global hash tables for hubs
+
     const auto& hubs = hub_index(d, g);
     if (hubs.count != static_cast<i64>(cnt[5])) fail(GP_ERUNTIME, "hub index disagrees with degree classes");
     i64 table_total = 0;
@@ -323,6 +324,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         fetch(d, &table_total, reinterpret_cast<i64*>(sc + 4), 1);
         w.partials.ensure(d, static_cast<size_t>(std::max<i64>(table_total / kSlotTile, hubs.chunks)));
         w.table.ensure(d, static_cast<size_t>(table_total));
+
         GP_CUDA(cudaMemsetAsync(w.table.get(), 0, table_total * sizeof(HubSlot), d.stream));
     }
 
@@ -382,11 +384,14 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
             launch(d, "affinity_block_hash_kernel", affinity_block_hash_kernel<O, W>, static_cast<int>(cnt[4]), kThreads, kLargeSlots * 12, 
                 cnt[4], class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
         if (cnt[5]) {
+            d.prof_bytes("hub_insert_kernel", static_cast<double>(class_edges[5]) * (4 + 4 + (ew ? sizeof(W) : 0)) +
+                                                  static_cast<double>(hubs.chunks) * sizeof(Chunk));
+            d.prof_bytes("hub_candidates_kernel", static_cast<double>(table_total) * sizeof(HubSlot));
             launch(d, "hub_insert_kernel", hub_insert_kernel<O, W>, static_cast<int>(hubs.chunks), kThreads, 0,
                    hubs.chunk.get(), nbr, ew, clusters, p, w.table_off.get(), w.table.get(), d.err);
             launch(d, "hub_candidates_kernel", hub_candidates_kernel<W>, static_cast<int>(table_total / kSlotTile),
                    kThreads, 0, hubs.count, hubs.list.get(), w.table_off.get(), w.table.get(), clusters, p,
-                   w.partials.get());
+                   w.partials.get(), i64{0});
             launch(d, "hub_finalize_kernel", hub_finalize_kernel<W>, blocks_for(hubs.count, kThreads), kThreads, 0,
                    hubs.count, hubs.list.get(), w.table_off.get(), w.partials.get(), clusters, vw, cw, p, so);
         }
@@ -562,14 +567,18 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     // row classes
     Buf<u64> rk(d, static_cast<size_t>(coarse_n)), rk_alt(d, static_cast<size_t>(coarse_n));
     Buf<i32> rl(d, static_cast<size_t>(coarse_n)), rl_alt(d, static_cast<size_t>(coarse_n));
-    Buf<u32> rc(d, 4);
+    Buf<u64> rc(d, 8);
     rc.zero(d);
     launch(d, "row_class_kernel", row_class_kernel, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n,
            temp_off.get(), static_cast<i64>(seg_smem_capacity<W>()), rk.get(), rl.get(), rc.get());
     GP_LAUNCH();
     radix_sort<u64, i32>(d, rk.get(), rl.get(), rk_alt.get(), rl_alt.get(), coarse_n, 0, 8);
-    u32 rcnt[4];
-    fetch(d, rcnt, rc.get(), 4);
+    u64 rcnt[8];
+    fetch(d, rcnt, rc.get(), 8);
+    // segment kernels read and write each scattered entry once (target + weight)
+    d.prof_bytes("segment_warp_kernel", 2.0 * static_cast<double>(rcnt[5]) * (4 + sizeof(W)));
+    d.prof_bytes("segment_smem_kernel", 2.0 * static_cast<double>(rcnt[6]) * (4 + sizeof(W)));
+    d.prof_bytes("segment_global_kernel", 2.0 * static_cast<double>(rcnt[7]) * (4 + sizeof(W)));
     const i64 c1 = rcnt[0], c2 = c1 + rcnt[1], c3 = c2 + rcnt[2];
     Buf<i64> row_len(d, static_cast<size_t>(coarse_n) + 1);
     row_len.zero(d);
@@ -971,6 +980,11 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         if (c0.movers == 0) return 0;
         const bool rebuild = lp && c0.mover_degree > g.m / 8;
         if (!rebuild) {
+            // per mover: offsets, label and target; per mover edge: neighbour,
+            // weight, the neighbour's label and two read-modify-writes of the cache
+            d.prof_bytes("apply_cache_cut_kernel",
+                         static_cast<double>(c0.movers) * (2 * sizeof(O) + 4 + 4 + 4) +
+                             static_cast<double>(c0.mover_degree) * (4 + 4 + (ew ? sizeof(W) : 0) + 4 * sizeof(C)));
             launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, c0.movers * 32),
                    kThreads, 0, w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache,
                    ctr);
@@ -1226,12 +1240,14 @@ void uncoarsen(Device& d, Hierarchy<T>& h, Buf<i32>& labels, const Opts& o, u64 
 // Input preparation: upload, narrowing and validation on the GPU with the
 // rules and messages of src/graph.cpp:47-190.
 // ---------------------------------------------------------------------------
-template <typename O>
-__global__ void narrow_offsets_kernel(i64 n, const i64* in, O* out, i64 m, u32* err) {
+// Offsets narrowed to the width's type and shifted down by `base` (the first
+// edge of an instance inside a packed multi-graph CSR; 0 otherwise).
+template <typename I, typename O>
+__global__ void narrow_offsets_kernel(i64 n, const I* in, i64 base, O* out, i64 m, u32* err) {
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i > n) return;
-    const i64 x = in[i];
-    if (x < 0 || x > m || (i > 0 && x < in[i - 1])) set_error(err, kErrBadInput);
+    const i64 x = static_cast<i64>(in[i]) - base;
+    if (x < 0 || x > m || (i > 0 && x < static_cast<i64>(in[i - 1]) - base)) set_error(err, kErrBadInput);
     out[i] = static_cast<O>(x);
 }
 
@@ -1277,8 +1293,11 @@ __global__ void symmetry_kernel(i64 n, const O* off, const i32* nbr, const W* ew
     }
 }
 
+// `gi` describes the graph to partition; for one instance of a packed CSR its
+// pointers are already advanced to the instance and `base` is the value of
+// its first offset, which is subtracted from every offset.
 template <typename T>
-void prepare_graph(Device& d, const gp_graph* gi, DGraph<T>& g, bool verify) {
+void prepare_graph(Device& d, const gp_graph* gi, DGraph<T>& g, bool verify, i64 base = 0) {
     using O = typename T::O;
     using W = typename T::W;
     if (!gi) fail(GP_EINVAL, "null graph");
@@ -1296,31 +1315,61 @@ void prepare_graph(Device& d, const gp_graph* gi, DGraph<T>& g, bool verify) {
     g.m = m;
     // Device input in the width's own types is used in place (borrowed):
     // a resident graph is partitioned without a copy.
-    const bool borrow = on_dev && !gi->index64;
-    if (borrow) {
-        g.off.borrow(static_cast<O*>(const_cast<void*>(gi->offsets)), static_cast<size_t>(n) + 1);
-        g.nbr.borrow(static_cast<i32*>(const_cast<void*>(gi->neighbors)), static_cast<size_t>(m));
-    } else {
-        g.off = Buf<O>(d, static_cast<size_t>(n) + 1);
-        g.nbr = Buf<i32>(d, static_cast<size_t>(std::max<i64>(m, 1)));
-    }
-    if (borrow) {
-    } else if (gi->index64) {
-        Buf<i64> tmp(d, static_cast<size_t>(std::max<i64>(n + 1, m)));
-        GP_CUDA(cudaMemcpyAsync(tmp.get(), gi->offsets, (n + 1) * sizeof(i64), kind, d.stream));
-        launch(d, "narrow_offsets_kernel", narrow_offsets_kernel<O>, blocks_for(n + 1, kThreads), kThreads, 0, n, tmp.get(), g.off.get(), m, d.err);
-        GP_LAUNCH();
-        if (m) {
-            GP_CUDA(cudaMemcpyAsync(tmp.get(), gi->neighbors, m * sizeof(i64), kind, d.stream));
-            launch(d, "narrow_neighbors_kernel", narrow_neighbors_kernel, stride_grid(d, m), kThreads, 0, m, tmp.get(), g.nbr.get(), n, d.err);
-            GP_LAUNCH();
+    // index64: 0 = arrays in the width's types, 1 = int64 offsets and
+    // neighbours (the reference's file arrays), 2 = int64 offsets with int32
+    // neighbours (a packed multi-graph CSR).  Device arrays in the width's
+    // own types are used in place (borrowed): a resident graph is partitioned
+    // without a copy.
+    if (gi->index64 < 0 || gi->index64 > 2) fail(GP_EINVAL, "invalid index width");
+    const bool nbr64 = gi->index64 == 1;
+    const bool borrow_off = on_dev && gi->index64 == 0 && base == 0;
+    const bool borrow_nbr = on_dev && !nbr64;
+    if (borrow_off) g.off.borrow(static_cast<O*>(const_cast<void*>(gi->offsets)), static_cast<size_t>(n) + 1);
+    else g.off = Buf<O>(d, static_cast<size_t>(n) + 1);
+    if (borrow_nbr) g.nbr.borrow(static_cast<i32*>(const_cast<void*>(gi->neighbors)), static_cast<size_t>(m));
+    else g.nbr = Buf<i32>(d, static_cast<size_t>(std::max<i64>(m, 1)));
+    // device input is narrowed in place; host input goes through one staging buffer
+    Buf<i64> stage;
+    if (!on_dev && (gi->index64 != 0 || base != 0))
+        stage = Buf<i64>(d, static_cast<size_t>(std::max<i64>(n + 1, nbr64 ? m : 0)));
+    if (!borrow_off) {
+        if (gi->index64 != 0) {
+            const i64* src = static_cast<const i64*>(gi->offsets);
+            if (!on_dev) {
+                GP_CUDA(cudaMemcpyAsync(stage.get(), gi->offsets, (n + 1) * sizeof(i64), kind, d.stream));
+                src = stage.get();
+            }
+            launch(d, "narrow_offsets_kernel", narrow_offsets_kernel<i64, O>, blocks_for(n + 1, kThreads), kThreads,
+                   0, n, src, base, g.off.get(), m, d.err);
+        } else if (base != 0) {
+            const O* src = static_cast<const O*>(gi->offsets);
+            if (!on_dev) {
+                GP_CUDA(cudaMemcpyAsync(stage.get(), gi->offsets, (n + 1) * sizeof(O), kind, d.stream));
+                src = reinterpret_cast<const O*>(stage.get());
+            }
+            launch(d, "narrow_offsets_kernel", narrow_offsets_kernel<O, O>, blocks_for(n + 1, kThreads), kThreads, 0,
+                   n, src, base, g.off.get(), m, d.err);
+        } else {
+            GP_CUDA(cudaMemcpyAsync(g.off.get(), gi->offsets, (n + 1) * sizeof(O), kind, d.stream));
         }
-    } else {
-        GP_CUDA(cudaMemcpyAsync(g.off.get(), gi->offsets, (n + 1) * sizeof(O), kind, d.stream));
-        if (m) GP_CUDA(cudaMemcpyAsync(g.nbr.get(), gi->neighbors, m * sizeof(i32), kind, d.stream));
+        GP_LAUNCH();
+    }
+    if (!borrow_nbr && m) {
+        if (nbr64) {
+            const i64* src = static_cast<const i64*>(gi->neighbors);
+            if (!on_dev) {
+                GP_CUDA(cudaMemcpyAsync(stage.get(), gi->neighbors, m * sizeof(i64), kind, d.stream));
+                src = stage.get();
+            }
+            launch(d, "narrow_neighbors_kernel", narrow_neighbors_kernel, stride_grid(d, m), kThreads, 0, m, src,
+                   g.nbr.get(), n, d.err);
+            GP_LAUNCH();
+        } else {
+            GP_CUDA(cudaMemcpyAsync(g.nbr.get(), gi->neighbors, m * sizeof(i32), kind, d.stream));
+        }
     }
     launch(d, "check_offsets_kernel", check_offsets_kernel<O>, blocks_for(n + 1, kThreads), kThreads, 0, n, g.off.get(), m, d.err);
-    if (!gi->index64 && m) launch(d, "check_neighbors_kernel", check_neighbors_kernel, stride_grid(d, m), kThreads, 0, m, g.nbr.get(), n, d.err);
+    if (!nbr64 && m) launch(d, "check_neighbors_kernel", check_neighbors_kernel, stride_grid(d, m), kThreads, 0, m, g.nbr.get(), n, d.err);
     GP_LAUNCH();
     g.unit_ew = gi->edge_weights == nullptr;
     g.unit_vw = gi->vertex_weights == nullptr;
@@ -1652,8 +1701,14 @@ gp_status gp_partition_capacity(uint64_t total, int parts, double ratio, uint64_
     return guarded(nullptr, [&] { *out = gp::partition_capacity(total, parts, ratio); });
 }
 
-gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* options, int32_t* labels,
-                       gp_report* report) {
+}  // extern "C"
+
+namespace {
+
+// The whole pipeline on one graph; `graph` may be a view of one instance of a
+// packed CSR, whose offsets start at `base` instead of 0.
+gp_status partition_impl(gp_ctx* ctx, const gp_graph* graph, gp::i64 base, const gp_options* options,
+                         int32_t* labels, gp_report* report) {
     if (!ctx) return GP_EINVAL;
     return guarded(ctx, [&] {
         GP_CUDA(cudaSetDevice(ctx->dev.device));
@@ -1669,7 +1724,7 @@ gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* opt
             gp::partition_capacity(static_cast<gp::u64>(graph->n), o.parts, o.ratio);
             const auto prep_start = gp::Clock::now();
             gp::DGraph<T> g;
-            gp::prepare_graph<T>(d, graph, g, o.verify);
+            gp::prepare_graph<T>(d, graph, g, o.verify, base);
             d.sync();
             rep.prepare_seconds = gp::seconds_since(prep_start);
             // algorithm_total_seconds scope (app/partition_main.cu:67-93)
@@ -1734,6 +1789,77 @@ gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* opt
             }
         });
         if (report) *report = rep;
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* options, int32_t* labels,
+                       gp_report* report) {
+    return partition_impl(ctx, graph, 0, options, labels, report);
+}
+
+gp_status gp_partition_range(gp_ctx* ctx, const gp_graph* packed, int64_t vertex_begin, int64_t vertex_end,
+                             const gp_options* options, int32_t* labels, gp_report* report) {
+    if (!ctx) return GP_EINVAL;
+    gp_graph view{};
+    gp::i64 base = 0;
+    const gp_status s = guarded(ctx, [&] {
+        if (!packed) gp::fail(GP_EINVAL, "null graph");
+        if (vertex_begin < 0 || vertex_end < vertex_begin || vertex_end > packed->n)
+            gp::fail(GP_EINVAL, "instance range outside the packed graph");
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        const bool wide = packed->index64 || packed->width == GP_WIDTH_BIG;
+        const size_t osize = wide ? 8 : 4;
+        const size_t isize = packed->index64 == 1 ? 8 : 4;
+        const size_t wsize = packed->width == GP_WIDTH_BIG ? 8 : 4;
+        const auto* off = static_cast<const unsigned char*>(packed->offsets);
+        auto read_offset = [&](gp::i64 v) -> gp::i64 {
+            unsigned char raw[8] = {};
+            if (packed->memory == GP_MEMORY_DEVICE)
+                GP_CUDA(cudaMemcpy(raw, off + v * osize, osize, cudaMemcpyDeviceToHost));
+            else
+                std::memcpy(raw, off + v * osize, osize);
+            if (wide) { int64_t x; std::memcpy(&x, raw, 8); return x; }
+            int32_t x;
+            std::memcpy(&x, raw, 4);
+            return x;
+        };
+        const gp::i64 first = read_offset(vertex_begin), last = read_offset(vertex_end);
+        if (first < 0 || last < first || last > packed->m)
+            gp::fail(GP_ERUNTIME, "weighted CSR shape is invalid (offsets not monotone or neighbor out of range)");
+        base = first;
+        view = *packed;
+        view.n = vertex_end - vertex_begin;
+        view.m = last - first;
+        view.offsets = off + vertex_begin * osize;
+        view.neighbors = static_cast<const unsigned char*>(packed->neighbors) + base * isize;
+        if (packed->edge_weights)
+            view.edge_weights = static_cast<const unsigned char*>(packed->edge_weights) + base * wsize;
+        if (packed->vertex_weights)
+            view.vertex_weights = static_cast<const unsigned char*>(packed->vertex_weights) + vertex_begin * wsize;
+    });
+    if (s != GP_OK) return s;
+    return partition_impl(ctx, &view, base, options, labels, report);
+}
+
+gp_status gp_ctx_memory(gp_ctx* ctx, uint64_t* live, uint64_t* cached, uint64_t* peak, int reset_peak) {
+    if (!ctx) return GP_EINVAL;
+    auto& d = ctx->dev;
+    if (live) *live = d.live_bytes;
+    if (cached) *cached = d.cached_bytes;
+    if (peak) *peak = d.peak_bytes;
+    if (reset_peak) d.peak_bytes = d.live_bytes;
+    return GP_OK;
+}
+
+gp_status gp_ctx_trim(gp_ctx* ctx) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        ctx->dev.release_cached();
     });
 }
 

@@ -35,6 +35,16 @@ def _lib():
                                     i64p, i64p]
         lib.gp_gen_rgg.argtypes = [ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, ctypes.c_char_p,
                                    ctypes.c_char_p, i64p, i64p]
+        vp = ctypes.c_void_p
+        lib.gp_gen_grid2d_new.argtypes = [ctypes.c_int64, ctypes.c_int64, i64p, i64p]
+        lib.gp_gen_grid2d_new.restype = vp
+        lib.gp_gen_rmat_new.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_uint64, i64p, i64p]
+        lib.gp_gen_rmat_new.restype = vp
+        lib.gp_gen_rgg_new.argtypes = [ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, i64p, i64p]
+        lib.gp_gen_rgg_new.restype = vp
+        lib.gp_gen_copy.argtypes = [vp, vp, vp, ctypes.c_int]
+        lib.gp_gen_free.argtypes = [vp]
         _LIB = lib
     return _LIB
 
@@ -92,6 +102,93 @@ def load(indptr: Path, indices: Path) -> tuple[np.ndarray, np.ndarray]:
     off = np.fromfile(indptr, dtype=np.int64)
     idx = np.memmap(indices, dtype=np.int64, mode="r") if os.path.getsize(indices) else np.zeros(0, np.int64)
     return off, idx
+
+
+def _in_memory(make, *args) -> tuple[np.ndarray, np.ndarray]:
+    """Run an in-memory generator: int64 offsets and int32 neighbours."""
+    L = _lib()
+    n, m = ctypes.c_int64(), ctypes.c_int64()
+    h = make(*args, ctypes.byref(n), ctypes.byref(m))
+    if not h:
+        raise RuntimeError(L.gp_gen_last_error().decode())
+    try:
+        off = np.empty(n.value + 1, np.int64)
+        nbr = np.empty(m.value, np.int32)
+        if L.gp_gen_copy(h, off.ctypes.data, nbr.ctypes.data, 4) != 0:
+            raise RuntimeError(L.gp_gen_last_error().decode())
+    finally:
+        L.gp_gen_free(h)
+    return off, nbr
+
+
+def rgg_csr(n: int, mean_degree: float = 10.0, seed: int = 7):
+    radius = math.sqrt(mean_degree / (math.pi * n))
+    return _in_memory(_lib().gp_gen_rgg_new, n, radius, seed)
+
+
+def grid2d_csr(nx: int, ny: int):
+    return _in_memory(_lib().gp_gen_grid2d_new, nx, ny)
+
+
+def rmat_csr(scale: int, edge_factor: int = 16, seed: int = 1):
+    return _in_memory(_lib().gp_gen_rmat_new, scale, edge_factor, 0.57, 0.19, 0.19, seed)
+
+
+def rgg_batch(count: int = 512, seed: int = 7, n_lo: float = 1e3, n_hi: float = 1e6,
+              mean_degree: float = 10.0, parts=(2, 4, 8, 16, 32)):
+    """The batched workload: `count` random geometric graphs in the unit
+    square, n log-uniform in [n_lo, n_hi], radius sqrt(mean_degree/(pi n)),
+    each with k drawn uniformly from `parts`; all drawn from one seeded
+    stream.  Returns (packed offsets int64, neighbours int32, vertex offsets,
+    ks), cached on disk by parameters."""
+    name = f"rgg_batch_{count}_{seed}_{n_lo:g}_{n_hi:g}_{mean_degree:g}"
+    root = cache_dir() / name
+    files = [root / f for f in ("off.npy", "nbr.npy", "vo.npy", "ks.npy")]
+    if all(f.exists() for f in files):
+        return tuple(np.load(f) for f in files)
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(math.log(n_lo), math.log(n_hi), count)).astype(np.int64)
+    ks = rng.choice(np.asarray(parts, np.int32), count)
+    offs, nbrs = [], []
+    for i, n in enumerate(ns):
+        off, nbr = rgg_csr(int(n), mean_degree, seed * 1_000_003 + i)
+        offs.append(off)
+        nbrs.append(nbr)
+    vo = np.zeros(count + 1, np.int64)
+    vo[1:] = np.cumsum(ns)
+    packed_off = np.zeros(int(vo[-1]) + 1, np.int64)
+    base = 0
+    for i, off in enumerate(offs):
+        packed_off[vo[i]:vo[i + 1] + 1] = off + base
+        base += int(off[-1])
+    nbr = np.concatenate(nbrs) if nbrs else np.zeros(0, np.int32)
+    root.mkdir(parents=True, exist_ok=True)
+    for f, a in zip(files, (packed_off, nbr, vo, ks)):
+        np.save(f, a)
+    return packed_off, nbr, vo, ks
+
+
+def serving_mix(count: int, seed: int = 11, n_lo: float = 1e4, n_hi: float = 4e6):
+    """Request graphs of the serving workload: each drawn uniformly from
+    {2D grid, RGG mean degree 10, RMAT edge factor 16} with n log-uniform in
+    [n_lo, n_hi] and k uniform in [2, 32].  A grid gets side round(sqrt(n)),
+    an RMAT graph scale round(log2 n).  Returns a list of
+    (kind, offsets, neighbours, k)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        kind = ("grid", "rgg", "rmat")[int(rng.integers(3))]
+        n = float(np.exp(rng.uniform(math.log(n_lo), math.log(n_hi))))
+        k = int(rng.integers(2, 33))
+        if kind == "grid":
+            side = max(2, int(round(math.sqrt(n))))
+            off, nbr = grid2d_csr(side, side)
+        elif kind == "rgg":
+            off, nbr = rgg_csr(int(n), 10.0, seed * 1_000_003 + i)
+        else:
+            off, nbr = rmat_csr(max(2, int(round(math.log2(n)))), 16, seed * 1_000_003 + i)
+        out.append((kind, off, nbr, k))
+    return out
 
 
 def by_name(name: str) -> tuple[Path, Path]:

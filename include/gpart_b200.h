@@ -48,7 +48,8 @@ enum { GP_MEMORY_HOST = 0, GP_MEMORY_DEVICE = 1 };
  * copy, and must stay valid and unmodified during the call.  With index64 = 1
  * offsets and neighbours are the int64 arrays of the reference's input files
  * (src/graph.cpp:47-122); the library narrows and validates them on the GPU
- * with the reference's rules and messages.  NULL weights mean unit weights
+ * with the reference's rules and messages.  index64 = 2 means int64 offsets
+ * with int32 neighbours (the packed multi-graph layout).  NULL weights mean unit weights
  * (the reference's file input always has unit weights,
  * src/graph.cpp:117-118). */
 typedef struct gp_graph {
@@ -127,6 +128,23 @@ gp_status gp_partition_capacity(uint64_t total, int parts, double ratio, uint64_
  * from the uploaded, validated graph to device labels with scratch released. */
 gp_status gp_partition(gp_ctx* ctx, const gp_graph* graph, const gp_options* options,
                        int32_t* labels, gp_report* report);
+
+/* Packed multi-graph CSR.  `packed` holds several instances back to back:
+ * offsets has n_total+1 entries and indexes the concatenated neighbour (and
+ * weight) arrays, neighbour ids are local to their instance (0 <= id < the
+ * instance's vertex count).  This partitions the instance of vertices
+ * [vertex_begin, vertex_end) exactly as gp_partition would partition it on
+ * its own; `labels` points at that instance's labels (vertex_end -
+ * vertex_begin entries, host or device like the graph).  No counterpart in
+ * the reference, which takes one graph per process run. */
+gp_status gp_partition_range(gp_ctx* ctx, const gp_graph* packed, int64_t vertex_begin, int64_t vertex_end,
+                             const gp_options* options, int32_t* labels, gp_report* report);
+
+/* Device memory of the context's caching allocator: bytes in use, bytes
+ * cached for reuse, and the peak in use (optionally reset to the current
+ * value).  gp_ctx_trim returns the cached blocks to the driver. */
+gp_status gp_ctx_memory(gp_ctx* ctx, uint64_t* live, uint64_t* cached, uint64_t* peak, int reset_peak);
+gp_status gp_ctx_trim(gp_ctx* ctx);
 
 /* One SCLP aggregation (replaces gpart::aggregate, include/coarsen.hpp:88-92;
  * src/coarsen.cu:1661-1671).  map: n int32 (host).  cluster_size_factor and
@@ -216,6 +234,60 @@ gp_status gp_profile_enable(gp_ctx* ctx, int on);
  * bytes>" (bytes are recorded for the kernels whose traffic model is known,
  * else 0). */
 gp_status gp_profile_dump(gp_ctx* ctx, char* buffer, uint64_t capacity);
+
+/* ------------------------------------------------------------------------
+ * Serving and batching (no counterpart in the reference).
+ *
+ * A server owns `slots` contexts on one device, each with its own stream,
+ * memory pool and host worker thread.  Submitted requests wait in a FIFO
+ * queue and are admitted in arrival order whenever a slot is idle and the
+ * projected device footprint (gp_footprint_bytes) of the running requests
+ * plus the next one fits in `memory_budget`; their work overlaps on the
+ * device.  Each request runs the same pipeline as gp_partition, so its result
+ * does not depend on the other requests (bit-identical when
+ * options.deterministic is set).  The graph arrays and `labels` of a request
+ * must stay valid until gp_server_wait returns for it.
+ * ---------------------------------------------------------------------- */
+typedef struct gp_server gp_server;
+
+typedef struct gp_request_info {
+    int32_t status;
+    int32_t slot;                 /* slot that ran the request */
+    double queued_seconds;        /* submit -> admitted */
+    double service_seconds;       /* admitted -> labels written */
+    double latency_seconds;       /* submit -> labels written */
+    uint64_t footprint_bytes;     /* projection used for admission */
+    char message[192];            /* failure message, "" on success */
+} gp_request_info;
+
+/* Projected peak device bytes of one partition (an upper bound of the
+ * library's own allocations; caller-owned device input is not counted). */
+uint64_t gp_footprint_bytes(int64_t n, int64_t m, int32_t parts, int32_t width, int32_t index64_host);
+
+gp_status gp_server_create(int device, int32_t slots, uint64_t memory_budget, gp_server** out);
+/* Waits for every admitted and queued request, then releases the slots. */
+void gp_server_destroy(gp_server* server);
+const char* gp_server_error(const gp_server* server);
+/* Queue one graph; GP_ENOMEM if its projection alone exceeds the budget. */
+gp_status gp_server_submit(gp_server* server, const gp_graph* graph, const gp_options* options, int32_t* labels,
+                           uint64_t* ticket);
+/* Queue one instance of a packed CSR (see gp_partition_range). */
+gp_status gp_server_submit_range(gp_server* server, const gp_graph* packed, int64_t vertex_begin,
+                                 int64_t vertex_end, const gp_options* options, int32_t* labels, uint64_t* ticket);
+gp_status gp_server_poll(gp_server* server, uint64_t ticket, int32_t* done);
+/* Blocks until the request is done, returns its status and releases the
+ * ticket. */
+gp_status gp_server_wait(gp_server* server, uint64_t ticket, gp_report* report, gp_request_info* info);
+
+/* Partitions every instance of a packed CSR (vertex_offsets: count+1 host
+ * entries, instance i = vertices [vertex_offsets[i], vertex_offsets[i+1]))
+ * on the server's slots, largest instances first.  options, reports and
+ * statuses have `count` entries (options NULL = defaults; reports/statuses
+ * may be NULL); labels has n_total entries.  Returns the first failing
+ * instance's status (details in gp_server_error). */
+gp_status gp_partition_batch(gp_server* server, const gp_graph* packed, int32_t count,
+                             const int64_t* vertex_offsets, const gp_options* options, int32_t* labels,
+                             gp_report* reports, int32_t* statuses);
 
 #ifdef __cplusplus
 }

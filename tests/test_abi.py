@@ -111,3 +111,62 @@ def test_generators_deterministic(tmp_path, monkeypatch):
 def test_grid_sizes():
     off, idx = graphs.load(*graphs.grid2d(256, 256))
     assert len(off) - 1 == 65536 and len(idx) == 261120
+
+
+def symmetric_simple(off, idx):
+    src = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    key = np.sort(src * (len(off) - 1) + idx)
+    return (src != idx).all() and np.array_equal(key, np.sort(idx.astype(np.int64) * (len(off) - 1) + src)) \
+        and (np.diff(key) > 0).all()
+
+
+def test_in_memory_generators_match_files(tmp_path, monkeypatch):
+    monkeypatch.setenv("GP_GRAPH_CACHE", str(tmp_path))
+    off, idx = graphs.load(*graphs.rmat(10))
+    off2, idx2 = graphs.rmat_csr(10, 16, 1)
+    assert np.array_equal(off, off2) and np.array_equal(np.asarray(idx), idx2)
+    a = graphs.rgg_csr(5000, 10.0, 3)
+    b = graphs.rgg_csr(5000, 10.0, 3)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert symmetric_simple(*a) and symmetric_simple(*graphs.grid2d_csr(9, 7))
+
+
+def test_packed_graph_layout():
+    gs = [graphs.grid2d_csr(3, 4), graphs.rgg_csr(200, 6.0, 1), (np.zeros(4, np.int64), np.zeros(0, np.int32))]
+    p = hb.PackedGraph.pack(gs)
+    assert p.count == 3 and p.n == sum(len(o) - 1 for o, _ in gs) and p.m == sum(len(x) for _, x in gs)
+    assert (np.diff(p.off) >= 0).all() and p.off[0] == 0 and p.off[-1] == p.m
+    for i, (off, nbr) in enumerate(gs):
+        o2, n2 = p.instance(i)
+        assert np.array_equal(o2, off) and np.array_equal(n2, nbr)
+    d = p.desc()
+    assert d.index64 == 2 and d.n == p.n and d.m == p.m
+
+
+def test_rgg_batch_shape(tmp_path, monkeypatch):
+    monkeypatch.setenv("GP_GRAPH_CACHE", str(tmp_path))
+    off, nbr, vo, ks = graphs.rgg_batch(count=6, seed=3, n_lo=100, n_hi=2000)
+    assert len(vo) == 7 and vo[-1] == len(off) - 1 and off[-1] == len(nbr)
+    sizes = np.diff(vo)
+    assert (sizes >= 100).all() and (sizes <= 2000).all()
+    assert set(ks.tolist()) <= {2, 4, 8, 16, 32}
+    p = hb.PackedGraph(off, nbr, vo)
+    for i in range(6):
+        assert symmetric_simple(*p.instance(i))
+    again = graphs.rgg_batch(count=6, seed=3, n_lo=100, n_hi=2000)
+    assert all(np.array_equal(x, y) for x, y in zip((off, nbr, vo, ks), again))
+
+
+def test_serving_mix_kinds():
+    mix = graphs.serving_mix(6, seed=11, n_lo=1e3, n_hi=4e3)
+    assert len(mix) == 6 and {k for k, *_ in mix} <= {"grid", "rgg", "rmat"}
+    for kind, off, nbr, k in mix:
+        assert 2 <= k <= 32 and symmetric_simple(off, nbr)
+
+
+def test_footprint_projection_is_monotone():
+    base = hb.footprint_bytes(1 << 20, 16 << 20, 8)
+    assert hb.footprint_bytes(1 << 21, 16 << 20, 8) > base
+    assert hb.footprint_bytes(1 << 20, 32 << 20, 8) > base
+    assert hb.footprint_bytes(1 << 20, 16 << 20, 32) > base
+    assert hb.footprint_bytes(1 << 20, 16 << 20, 8, hb.BIG) > base
