@@ -60,42 +60,79 @@ __global__ void hub_fill_kernel(i64 n, const O* off, const i64* hub_pos, const i
 // ---------------------------------------------------------------------------
 // SCLP affinity of hubs: chunked insertion into per-hub global tables with
 // warp-level pre-aggregation (__match_any_sync on the cluster id), then a
-// candidate pass over 2048-slot tiles (tables are power-of-two sized and at
-// least 8192 slots, so tiles never straddle two tables), then a per-hub
-// finalisation that merges the tiles and decodes the proposal.
+// candidate pass over kSlotTile-slot tiles (table sizes are multiples of the
+// tile, so tiles never straddle two tables), then a per-hub finalisation that
+// merges the tiles and decodes the proposal.
 // ---------------------------------------------------------------------------
-// One 16-byte slot holds key and value, so an insert or a read touches one
-// sector; key 0 is empty (cluster c is stored as c + 1), so a table is
-// cleared by a memset.
+// A slot holds key and value in one sector; key 0 is empty (cluster c is
+// stored as c + 1), so a table is cleared by a memset.  Levels whose total
+// edge weight fits in 32 bits use 8-byte slots (no per-cluster sum can
+// overflow), others 16-byte slots; tables are about 1.3x the hub's degree,
+// so the 8-byte form keeps the level-0 tables of large power-law graphs
+// several times smaller and mostly resident in L2.
 struct HubSlot {
     u32 key;
     u32 pad;
     u64 val;
+    __device__ void add(u64 w) { atomic_add_u64(&val, w); }
+    __device__ u64 value() const { return val; }
 };
 
-__device__ __forceinline__ void slot_insert(HubSlot* table, u32 mask, i32 c, u64 w, u32* err) {
+struct HubSlot32 {
+    u32 key;
+    u32 val;
+    __device__ void add(u64 w) { atomicAdd(&val, static_cast<u32>(w)); }
+    __device__ u64 value() const { return val; }
+};
+
+constexpr i64 kSlotTile = 1024;
+
+// Table size of a hub: at least 1.3x its degree (load factor <= 0.77 even
+// if every neighbour is in a different cluster), rounded up to whole tiles.
+template <typename O>
+struct HubTableSize {
+    const i32* list;
+    const O* off;
+    i64 count;
+    __device__ i64 operator()(i64 i) const {
+        if (i >= count) return 0;
+        const i32 v = list[i];
+        const i64 d = static_cast<i64>(off[v + 1]) - off[v];
+        const i64 want = d + (d * 3 + 9) / 10;
+        return (want + kSlotTile - 1) / kSlotTile * kSlotTile;
+    }
+};
+
+// Fixed-point range reduction of the hash onto [0, size) (size < 2^32).
+__device__ __forceinline__ u32 slot_of(i32 c, u32 size) {
+    return static_cast<u32>((static_cast<u64>(mix32(static_cast<u32>(c))) * size) >> 32);
+}
+
+template <typename S>
+__device__ __forceinline__ void slot_insert(S* table, u32 size, i32 c, u64 w, u32* err) {
     const u32 key = static_cast<u32>(c) + 1;
-    u32 slot = mix32(static_cast<u32>(c)) & mask;
-    for (u32 probe = 0; probe <= mask; ++probe) {
+    u32 slot = slot_of(c, size);
+    for (u32 probe = 0; probe < size; ++probe) {
         const u32 found = atomicCAS(&table[slot].key, 0u, key);
         if (found == 0u || found == key) {
-            atomic_add_u64(&table[slot].val, w);
+            table[slot].add(w);
             return;
         }
-        slot = (slot + 1) & mask;
+        if (++slot == size) slot = 0;
     }
     set_error(err, kErrTableFull);
 }
 
-template <typename O, typename W>
+template <typename O, typename W, typename S>
 __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
     const Chunk* __restrict__ chunks, const i32* __restrict__ nbr, const W* __restrict__ ew,
-    const i32* __restrict__ clusters, RoundParams p, const i64* __restrict__ table_off, HubSlot* table, u32* err) {
+    const i32* __restrict__ clusters, RoundParams p, const i64* __restrict__ table_off, S* table, u32* err) {
     const Chunk ch = chunks[blockIdx.x];
+    if (role_blocked(p.identity ? ch.v : clusters[ch.v], p)) return;   // no proposal: nothing to count
     const int lane = threadIdx.x & 31;
     const i64 t0 = table_off[ch.hub];
-    const u32 mask = static_cast<u32>(table_off[ch.hub + 1] - t0 - 1);
-    HubSlot* slots = table + t0;
+    const u32 size = static_cast<u32>(table_off[ch.hub + 1] - t0);
+    S* slots = table + t0;
     for (i64 base = ch.begin; base < ch.end; base += kThreads) {
         const i64 e = base + threadIdx.x;
         i32 c = -1;
@@ -109,22 +146,24 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
         }
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         u64 sum = 0;
+        if (ew == nullptr) {
+            sum = static_cast<u64>(__popc(peers));   // unit weights
+        } else {
 #pragma unroll
-        for (int s = 0; s < 32; ++s) {
-            const u64 pw = __shfl_sync(0xffffffffu, w, s);
-            if (peers & (1u << s)) sum += pw;
+            for (int s = 0; s < 32; ++s) {
+                const u64 pw = __shfl_sync(0xffffffffu, w, s);
+                if (peers & (1u << s)) sum += pw;
+            }
         }
-        if (c >= 0 && lane == __ffs(peers) - 1) slot_insert(slots, mask, c, sum, err);
+        if (c >= 0 && lane == __ffs(peers) - 1) slot_insert(slots, size, c, sum, err);
     }
 }
 
 struct HubPartial { u64 current, best, tie; };
 
-constexpr i64 kSlotTile = 2048;
-
-template <typename W>
+template <typename W, typename S>
 __global__ void __launch_bounds__(kThreads) hub_candidates_kernel(
-    i64 hubs, const i32* __restrict__ hub_list, const i64* __restrict__ table_off, HubSlot* table,
+    i64 hubs, const i32* __restrict__ hub_list, const i64* __restrict__ table_off, S* table,
     const i32* __restrict__ clusters, RoundParams p, HubPartial* partials, i64 tile_base) {
     __shared__ CandShared red;
     __shared__ int hub_sh;
@@ -142,12 +181,14 @@ __global__ void __launch_bounds__(kThreads) hub_candidates_kernel(
     const int h = hub_sh;
     const i32 v = hub_list[h];
     const i32 source = p.identity ? v : clusters[v];
+    if (role_blocked(source, p)) return;   // empty table, no proposal
     u64 current = 0, best = 0, tie = 0;
     for (i64 s = s0 + threadIdx.x; s < s0 + kSlotTile; s += kThreads) {
-        const HubSlot slot = table[s];
+        const S slot = table[s];
         if (slot.key) {
-            slot_candidate(static_cast<i32>(slot.key - 1), slot.val, static_cast<u32>(v), source, p, current, best, tie);
-            table[s] = {0u, 0u, 0ULL};
+            slot_candidate(static_cast<i32>(slot.key - 1), slot.value(), static_cast<u32>(v), source, p, current, best,
+                           tie);
+            table[s] = S{};
         }
     }
     block_candidate_reduce(current, best, tie, red);
@@ -352,6 +393,10 @@ __global__ void __launch_bounds__(kThreads) affinity_direct_warp_kernel(
     const i64 gid = (static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) >> 5;
     if (gid >= count) return;
     const i32 v = list[gid];
+    if (role_blocked(v, p)) {
+        if (lane == 0) out.target[v] = kInvalid;
+        return;
+    }
     u64 current = 0, best = 0, tie = 0;
     for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32)
         direct_candidate(v, nbr[e], static_cast<u64>(weight_at(ew, e)), p, best, tie);
@@ -365,6 +410,10 @@ __global__ void __launch_bounds__(kThreads) affinity_direct_block_kernel(
     const W* __restrict__ ew, const W* __restrict__ vw, const u64* __restrict__ cw, RoundParams p, SclpOut out) {
     __shared__ CandShared red;
     const i32 v = list[blockIdx.x];
+    if (role_blocked(v, p)) {
+        if (threadIdx.x == 0) out.target[v] = kInvalid;
+        return;
+    }
     u64 current = 0, best = 0, tie = 0;
     for (i64 e = static_cast<i64>(off[v]) + threadIdx.x; e < static_cast<i64>(off[v + 1]); e += kThreads)
         direct_candidate(v, nbr[e], static_cast<u64>(weight_at(ew, e)), p, best, tie);
@@ -379,6 +428,7 @@ __global__ void __launch_bounds__(kThreads) hub_direct_kernel(const Chunk* __res
                                                               RoundParams p, HubPartial* partials) {
     __shared__ CandShared red;
     const Chunk ch = chunks[blockIdx.x];
+    if (role_blocked(ch.v, p)) return;   // the hub's finalisation writes no proposal
     u64 current = 0, best = 0, tie = 0;
     for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads)
         direct_candidate(ch.v, nbr[e], static_cast<u64>(weight_at(ew, e)), p, best, tie);
@@ -403,35 +453,6 @@ __global__ void hub_chunk_finalize_kernel(i64 hubs, const i32* __restrict__ hub_
         if (better(q.best, q.tie, best, tie)) { best = q.best; tie = q.tie; }
     }
     decode_and_write(v, source, current, best, tie, p, vw, cw, out);
-}
-
-// Hub insertion with shared-memory pre-aggregation: a block first sums its
-// chunk per cluster in a 4096-slot shared table, then adds each distinct
-// cluster once to the hub's global table.
-constexpr int kChunkSlots = 4096;   // >= 2 * kChunkEdges
-
-template <typename O, typename W>
-__global__ void __launch_bounds__(kThreads) hub_insert_smem_kernel(
-    const Chunk* __restrict__ chunks, const i32* __restrict__ nbr, const W* __restrict__ ew,
-    const i32* __restrict__ clusters, RoundParams p, const i64* __restrict__ table_off, i32* table_keys,
-    u64* table_vals, u32* err) {
-    extern __shared__ unsigned char smem_raw[];
-    u64* svals = reinterpret_cast<u64*>(smem_raw);
-    i32* skeys = reinterpret_cast<i32*>(svals + kChunkSlots);
-    const Chunk ch = chunks[blockIdx.x];
-    for (int s = threadIdx.x; s < kChunkSlots; s += kThreads) { skeys[s] = -1; svals[s] = 0; }
-    __syncthreads();
-    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
-        const i32 u = nbr[e];
-        if (u == ch.v) continue;
-        table_insert(skeys, svals, kChunkSlots - 1, p.identity ? u : clusters[u], static_cast<u64>(weight_at(ew, e)),
-                     err);
-    }
-    __syncthreads();
-    const i64 t0 = table_off[ch.hub];
-    const u32 mask = static_cast<u32>(table_off[ch.hub + 1] - t0 - 1);
-    for (int s = threadIdx.x; s < kChunkSlots; s += kThreads)
-        if (skeys[s] >= 0) table_insert(table_keys + t0, table_vals + t0, mask, skeys[s], svals[s], err);
 }
 
 // Level-0 check of the reference's sorted-unique flag (src/coarsen.cu:44-70):

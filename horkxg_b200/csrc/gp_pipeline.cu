@@ -325,7 +325,8 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         w.partials.ensure(d, static_cast<size_t>(std::max<i64>(table_total / kSlotTile, hubs.chunks)));
         w.table.ensure(d, static_cast<size_t>(table_total));
 
-        GP_CUDA(cudaMemsetAsync(w.table.get(), 0, table_total * sizeof(HubSlot), d.stream));
+        GP_CUDA(cudaMemsetAsync(w.table.get(), 0, table_total * (sum32 ? sizeof(HubSlot32) : sizeof(HubSlot)),
+                                d.stream));
     }
 
     trace().mark(d, "agg.hub_tables", level);
@@ -349,7 +350,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
             d.prof_bytes("affinity_small_kernel", affinity_bytes(1, p.identity) + affinity_bytes(2, p.identity));
             d.prof_bytes("affinity_warp_hash_kernel", affinity_bytes(3, p.identity));
             d.prof_bytes("affinity_block_hash_kernel", affinity_bytes(4, p.identity));
-            d.prof_bytes("affinity_global_hash_kernel", affinity_bytes(5, p.identity));
+
         }
         if (cnt[1])
             launch(d, "affinity_small_kernel", affinity_small_kernel<8, O, W>, blocks_for(static_cast<i64>(cnt[1]) * 8, kThreads), kThreads, 0, 
@@ -386,12 +387,17 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         if (cnt[5]) {
             d.prof_bytes("hub_insert_kernel", static_cast<double>(class_edges[5]) * (4 + 4 + (ew ? sizeof(W) : 0)) +
                                                   static_cast<double>(hubs.chunks) * sizeof(Chunk));
-            d.prof_bytes("hub_candidates_kernel", static_cast<double>(table_total) * sizeof(HubSlot));
-            launch(d, "hub_insert_kernel", hub_insert_kernel<O, W>, static_cast<int>(hubs.chunks), kThreads, 0,
-                   hubs.chunk.get(), nbr, ew, clusters, p, w.table_off.get(), w.table.get(), d.err);
-            launch(d, "hub_candidates_kernel", hub_candidates_kernel<W>, static_cast<int>(table_total / kSlotTile),
-                   kThreads, 0, hubs.count, hubs.list.get(), w.table_off.get(), w.table.get(), clusters, p,
-                   w.partials.get(), i64{0});
+            auto hub_tables = [&](auto* table) {
+                using S = std::remove_pointer_t<decltype(table)>;
+                d.prof_bytes("hub_candidates_kernel", static_cast<double>(table_total) * sizeof(S));
+                launch(d, "hub_insert_kernel", hub_insert_kernel<O, W, S>, static_cast<int>(hubs.chunks), kThreads, 0,
+                       hubs.chunk.get(), nbr, ew, clusters, p, w.table_off.get(), table, d.err);
+                launch(d, "hub_candidates_kernel", hub_candidates_kernel<W, S>,
+                       static_cast<int>(table_total / kSlotTile), kThreads, 0, hubs.count, hubs.list.get(),
+                       w.table_off.get(), table, clusters, p, w.partials.get(), i64{0});
+            };
+            if (sum32) hub_tables(reinterpret_cast<HubSlot32*>(w.table.get()));
+            else hub_tables(w.table.get());
             launch(d, "hub_finalize_kernel", hub_finalize_kernel<W>, blocks_for(hubs.count, kThreads), kThreads, 0,
                    hubs.count, hubs.list.get(), w.table_off.get(), w.partials.get(), clusters, vw, cw, p, so);
         }

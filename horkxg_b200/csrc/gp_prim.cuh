@@ -28,6 +28,54 @@ __device__ __forceinline__ T warp_inclusive_sum(T v) {
     return v;
 }
 
+// Warp-cooperative walk over the edges of up to 32 rows, one row per lane
+// (first edge `begin`, `deg` edges, 0 for no row).  The rows' edges are laid
+// back to back in a virtual position space and visited 32 at a time, so short
+// rows leave no lane idle.  f(valid, owner, edge) is called by every lane in
+// every step (valid is false past the last edge, so f may use warp
+// collectives); owner is the lane whose row the edge belongs to and is
+// non-decreasing across the lanes of a step.
+template <typename F>
+__device__ __forceinline__ void warp_edge_walk(i64 begin, i64 deg, F&& f) {
+    const int lane = threadIdx.x & 31;
+    const i64 inc = warp_inclusive_sum(deg);
+    const i64 pre = inc - deg;
+    const i64 total = __shfl_sync(0xffffffffu, inc, 31);
+    for (i64 base = 0; base < total; base += 32) {
+        const i64 q = base + lane;
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+            const i64 probe = __shfl_sync(0xffffffffu, pre, lo + step);
+            if (probe <= q) lo += step;
+        }
+        const i64 my_pre = __shfl_sync(0xffffffffu, pre, lo);
+        const i64 my_begin = __shfl_sync(0xffffffffu, begin, lo);
+        f(q < total, lo, my_begin + (q - my_pre));
+    }
+}
+
+// Rows a warp takes at once in a warp_edge_walk loop over `count` rows: up to
+// 32 when there are many, down to one per warp when there are few (a walk
+// over fewer rows than warps would leave most warps idle).
+__device__ __forceinline__ int rows_per_warp(i64 count, i64 warps) {
+    const i64 g = count / (warps > 0 ? warps : 1);
+    return static_cast<int>(g < 1 ? 1 : (g > 32 ? 32 : g));
+}
+
+// Inclusive sum over runs of equal, non-decreasing `key` across the warp.
+template <typename T>
+__device__ __forceinline__ T warp_run_sum(T v, int key) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const T o = __shfl_up_sync(0xffffffffu, v, d);
+        const int ok = __shfl_up_sync(0xffffffffu, key, d);
+        if (lane >= d && ok == key) v += o;
+    }
+    return v;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

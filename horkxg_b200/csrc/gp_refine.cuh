@@ -144,40 +144,58 @@ __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i3
     }
 }
 
-// incremental_priority_filter (src/refine_incremental.cuh:48-67), warp per
-// proposer; movers are appended to `movers` and flagged.
+// incremental_priority_filter (src/refine_incremental.cuh:48-67); movers are
+// appended to `movers` and flagged.
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) priority_filter_kernel(
     const i32* __restrict__ list, const RefineCounters* ctr_in, const O* __restrict__ off,
     const i32* __restrict__ nbr, const W* __restrict__ ew, const PropRec* __restrict__ props, unsigned char* flags,
     i32* movers, RefineCounters* ctr) {
-    const int lane = threadIdx.x & 31;
+    // A warp takes up to 32 proposers and walks their edges together; each
+    // row's correction is summed in shared memory (hub rows: chunked kernel).
+    __shared__ long long corr_sh[kWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 count = ctr_in->proposers;
-    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
-    for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
-        const i32 v = list[i];
-        if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub: chunked kernel
-        const PropRec me = props[v];
-        const i32 s = me.label, t = me.target;
-        const i64 g = me.gain;
-        long long corr = 0;
-        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
-            const i32 u = nbr[e];
-            if (u == v) continue;
-            const PropRec o = props[u];
-            if (o.target < 0) continue;
-            if (!(o.gain > g || (o.gain == g && u < v))) continue;
-            const auto w = static_cast<long long>(weight_at(ew, e));
-            corr += w * ((o.target == t) - (o.target == s) - (o.label == t) + (o.label == s));
-        }
-        corr = warp_sum(corr);
-        if (lane == 0 && g + corr >= 0) {
+    const i64 warps = static_cast<i64>(gridDim.x) * kWarps;
+    const int G = rows_per_warp(count, warps);
+    for (i64 i0 = (static_cast<i64>(blockIdx.x) * kWarps + warp) * G; i0 < count; i0 += warps * G) {
+        const i64 i = i0 + lane;
+        const bool has = lane < G && i < count;
+        const i32 v = has ? list[i] : 0;
+        const i64 b = has ? static_cast<i64>(off[v]) : 0;
+        const i64 deg = has ? static_cast<i64>(off[v + 1]) - b : 0;
+        const bool hub = deg > kHubDegree;
+        const PropRec me = has ? props[v] : PropRec{0, -1, 0};
+        corr_sh[warp][lane] = 0;
+        __syncwarp();
+        warp_edge_walk(b, hub ? 0 : deg, [&](bool valid, int owner, i64 e) {
+            const i32 ov = __shfl_sync(0xffffffffu, v, owner);
+            const i32 s = __shfl_sync(0xffffffffu, me.label, owner);
+            const i32 t = __shfl_sync(0xffffffffu, me.target, owner);
+            const i64 g = __shfl_sync(0xffffffffu, me.gain, owner);
+            long long c = 0;
+            if (valid) {
+                const i32 u = nbr[e];
+                if (u != ov) {
+                    const PropRec o = props[u];
+                    if (o.target >= 0 && (o.gain > g || (o.gain == g && u < ov))) {
+                        const auto w = static_cast<long long>(weight_at(ew, e));
+                        c = w * ((o.target == t) - (o.target == s) - (o.label == t) + (o.label == s));
+                    }
+                }
+            }
+            const long long run = warp_run_sum(c, owner);
+            const int next = __shfl_down_sync(0xffffffffu, owner, 1);
+            if ((lane == 31 || next != owner) && run != 0) corr_sh[warp][owner] += run;
+            __syncwarp();
+        });
+        if (has && !hub && me.gain + corr_sh[warp][lane] >= 0) {
             flags[v] = 1;
             const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
             movers[slot] = v;
-            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree),
-                      static_cast<unsigned long long>(static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v])));
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree), static_cast<unsigned long long>(deg));
         }
+        __syncwarp();
     }
 }
 
@@ -187,28 +205,39 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
     const i32* __restrict__ movers, const RefineCounters* ctr_in, const O* __restrict__ off,
     const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
     const i32* __restrict__ targets, const unsigned char* __restrict__ flags, int k, C* cache, RefineCounters* ctr) {
+    // A warp takes up to 32 movers and walks their edges together (hub rows:
+    // chunked kernel).
     __shared__ long long sh[kWarps + 1];
     const int lane = threadIdx.x & 31;
     const i64 count = ctr_in->movers;
-    const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
+    const i64 warps = static_cast<i64>(gridDim.x) * kWarps;
+    const int G = rows_per_warp(count, warps);
     long long gain = 0;
-    for (i64 i = static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5); i < count; i += warps_total) {
-        const i32 v = movers[i];
-        if (static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]) > kHubDegree) continue;   // hub: chunked kernel
-        const i32 s = labels[v], t = targets[v];
-        for (i64 e = static_cast<i64>(off[v]) + lane; e < static_cast<i64>(off[v + 1]); e += 32) {
+    for (i64 i0 = (static_cast<i64>(blockIdx.x) * kWarps + (threadIdx.x >> 5)) * G; i0 < count; i0 += warps * G) {
+        const i64 i = i0 + lane;
+        const bool has = lane < G && i < count;
+        const i32 v = has ? movers[i] : 0;
+        const i64 b = has ? static_cast<i64>(off[v]) : 0;
+        i64 deg = has ? static_cast<i64>(off[v + 1]) - b : 0;
+        if (deg > kHubDegree) deg = 0;
+        const i32 s = has ? labels[v] : 0, t = has ? targets[v] : 0;
+        warp_edge_walk(b, deg, [&](bool valid, int owner, i64 e) {
+            const i32 ov = __shfl_sync(0xffffffffu, v, owner);
+            const i32 os = __shfl_sync(0xffffffffu, s, owner);
+            const i32 ot = __shfl_sync(0xffffffffu, t, owner);
+            if (!valid) return;
             const i32 u = nbr[e];
-            if (u == v) continue;
+            if (u == ov) return;
             const u64 w = static_cast<u64>(weight_at(ew, e));
-            cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
-            cache_add(&cache[static_cast<i64>(u) * k + t], w);
+            cache_add(&cache[static_cast<i64>(u) * k + os], 0ULL - w);
+            cache_add(&cache[static_cast<i64>(u) * k + ot], w);
             const bool fu = flags[u] != 0;
-            if (!fu || u > v) {
+            if (!fu || u > ov) {
                 const i32 lu = labels[u];
                 const i32 nn = fu ? targets[u] : lu;
-                gain += static_cast<long long>(w) * ((s != lu) - (t != nn));
+                gain += static_cast<long long>(w) * ((os != lu) - (ot != nn));
             }
-        }
+        });
     }
     gain = block_sum(gain, sh);
     if (threadIdx.x == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));

@@ -55,6 +55,13 @@ __device__ __forceinline__ bool is_mover(i32 c, const RoundParams& p) {
     return mix32(static_cast<u32>(c) ^ p.role_salt) < p.mover_threshold;
 }
 
+// With role filtering, a vertex whose own cluster is not a mover gets no
+// proposal whatever its affinities (sclp_decode_gain_kernel,
+// src/coarsen.cu:562-598), so its affinity pass is skipped altogether.
+__device__ __forceinline__ bool role_blocked(i32 source, const RoundParams& p) {
+    return p.filter && !is_mover(source, p);
+}
+
 // sclp_better_candidate, src/coarsen.cu:224-229
 __device__ __forceinline__ bool better(u64 a, u64 ta, u64 b, u64 tb) {
     return a > b || (a == b && a != 0 && ta > tb);
@@ -120,10 +127,11 @@ __global__ void __launch_bounds__(kThreads) affinity_small_kernel(
     const i64 gid = (static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) / G;
     const bool has_vertex = gid < count;
     const i32 v = has_vertex ? list[gid] : -1;
+    const i32 source = has_vertex ? (p.identity ? v : clusters[v]) : -1;
     bool valid = false;
     i32 c = -1;
     u64 w = 0;
-    if (has_vertex) {
+    if (has_vertex && !role_blocked(source, p)) {
         const i64 begin = off[v];
         const i64 deg = static_cast<i64>(off[v + 1]) - begin;
         if (lig < deg) {
@@ -149,7 +157,6 @@ __global__ void __launch_bounds__(kThreads) affinity_small_kernel(
         }
     }
     const bool leader = valid && lane == __ffs(peers) - 1;
-    const i32 source = has_vertex ? (p.identity ? v : clusters[v]) : -1;
     u64 current = 0, best = 0, tie = 0;
     if (leader) {
         if (c == source) {
@@ -199,11 +206,16 @@ __global__ void __launch_bounds__(kThreads) affinity_warp_hash_kernel(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 gid = static_cast<i64>(blockIdx.x) * kWarps + warp;
     if (gid >= count) return;
+    const i32 v = list[gid];
+    const i32 source = p.identity ? v : clusters[v];
+    if (role_blocked(source, p)) {
+        if (lane == 0) out.target[v] = kInvalid;
+        return;
+    }
     i32* keys = keys_all[warp];
     u64* vals = vals_all[warp];
     for (int s = lane; s < kMediumSlots; s += 32) { keys[s] = -1; vals[s] = 0; }
     __syncwarp();
-    const i32 v = list[gid];
     const i64 begin = off[v], end = off[v + 1];
     for (i64 e = begin + lane; e < end; e += 32) {
         const i32 u = nbr[e];
@@ -212,7 +224,6 @@ __global__ void __launch_bounds__(kThreads) affinity_warp_hash_kernel(
                      static_cast<u64>(weight_at(ew, e)), err);
     }
     __syncwarp();
-    const i32 source = p.identity ? v : clusters[v];
     u64 current = 0, best = 0, tie = 0;
     for (int s = lane; s < kMediumSlots; s += 32) slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
     group_reduce(current, best, tie, 32, 0xffffffffu);
@@ -247,6 +258,11 @@ __global__ void __launch_bounds__(kThreads) affinity_block_hash_kernel(
     const i64 gid = blockIdx.x;
     if (gid >= count) return;
     const i32 v = list[gid];
+    const i32 source = p.identity ? v : clusters[v];
+    if (role_blocked(source, p)) {
+        if (threadIdx.x == 0) out.target[v] = kInvalid;
+        return;
+    }
     const i64 begin = off[v], end = off[v + 1];
     int slots = 512;   // power of two >= 2 * degree (degree <= kHubDegree)
     while (slots < 2 * (end - begin) && slots < kLargeSlots) slots <<= 1;
@@ -259,43 +275,8 @@ __global__ void __launch_bounds__(kThreads) affinity_block_hash_kernel(
                      static_cast<u64>(weight_at(ew, e)), err);
     }
     __syncthreads();
-    const i32 source = p.identity ? v : clusters[v];
     u64 current = 0, best = 0, tie = 0;
     for (int s = threadIdx.x; s < slots; s += kThreads) slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
-    block_candidate_reduce(current, best, tie, red);
-    if (threadIdx.x == 0) decode_and_write(v, source, current, best, tie, p, vw, cw, out);
-}
-
-// Block per hub with a global hash table (power-of-two slots, >= 2 * degree)
-// at table_off[gid]; the table is left cleared for the next round.
-template <typename O, typename W>
-__global__ void __launch_bounds__(kThreads) affinity_global_hash_kernel(
-    i64 count, const i32* __restrict__ list, const O* __restrict__ off, const i32* __restrict__ nbr,
-    const W* __restrict__ ew, const W* __restrict__ vw, const i32* __restrict__ clusters,
-    const u64* __restrict__ cw, RoundParams p, SclpOut out, const i64* __restrict__ table_off,
-    i32* table_keys, u64* table_vals, u32* err) {
-    __shared__ CandShared red;
-    const i64 gid = blockIdx.x;
-    if (gid >= count) return;
-    const i64 t0 = table_off[gid];
-    const u32 mask = static_cast<u32>(table_off[gid + 1] - t0 - 1);
-    i32* keys = table_keys + t0;
-    u64* vals = table_vals + t0;
-    const i32 v = list[gid];
-    const i64 begin = off[v], end = off[v + 1];
-    for (i64 e = begin + threadIdx.x; e < end; e += kThreads) {
-        const i32 u = nbr[e];
-        if (u == v) continue;
-        table_insert(keys, vals, mask, p.identity ? u : clusters[u], static_cast<u64>(weight_at(ew, e)), err);
-    }
-    __syncthreads();
-    const i32 source = p.identity ? v : clusters[v];
-    u64 current = 0, best = 0, tie = 0;
-    for (u32 s = threadIdx.x; s <= mask; s += kThreads) {
-        slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
-        keys[s] = -1;
-        vals[s] = 0;
-    }
     block_candidate_reduce(current, best, tie, red);
     if (threadIdx.x == 0) decode_and_write(v, source, current, best, tie, p, vw, cw, out);
 }
@@ -329,24 +310,6 @@ __global__ void degree_class_kernel(i64 n, const O* off, u64* keys, i32* vals, u
     }
 }
 
-// Global hash table sizes for hubs: next power of two >= 2 * degree.
-template <typename O>
-struct HubTableSize {
-    const i32* list;
-    const O* off;
-    i64 count;
-    __device__ i64 operator()(i64 i) const {
-        if (i >= count) return 0;
-        const i32 v = list[i];
-        const i64 d = static_cast<i64>(off[v + 1]) - off[v];
-        // power of two >= 1.25 * degree, at least 4096 (a multiple of the
-        // 2048-slot candidate tile); rounds after the first see far fewer
-        // distinct clusters than neighbours
-        i64 s = 4096;
-        while (s < d + d / 4) s <<= 1;
-        return s;
-    }
-};
 
 
 // Level statistics: total / maximum vertex weight and degree-class counts.
