@@ -5,9 +5,10 @@
 //    degrees; a warp-batched pass scatters each fine row's (map[u], w) pairs
 //    into its coarse row's segment (internal edges become a sentinel);
 // 2. every segment is sorted by target and its runs of equal targets summed:
-//    a warp bitonic sort for segments of <= 32 entries, a shared-memory block
-//    radix sort for segments that fit shared memory, a global-memory block radix sort for
-//    larger (hub) segments;
+//    a warp bitonic sort in registers for segments of <= 32 entries, a warp
+//    radix sort in the warp's shared memory for <= 256, a block radix sort in
+//    shared memory sized to the segment class for <= 4096, and a block radix
+//    sort through global scratch for larger (hub) segments;
 // 3. row lengths are scanned into the coarse offsets and the unique entries
 //    copied out.
 //
@@ -24,6 +25,12 @@ namespace gp {
 // (plus the ranking scratch) stay under the 227 KB a block may use.
 template <typename W>
 __host__ __device__ constexpr int seg_smem_capacity() { return 4096; }
+constexpr int kWarpSegCap = 256;    // warp radix sort
+constexpr int kMidSegCap = 1024;    // block radix sort with a 1024-entry buffer
+
+// Row-size classes: 0 empty, 1 <= 32, 2 <= kWarpSegCap, 3 <= kMidSegCap,
+// 4 <= seg_smem_capacity, 5 larger.
+constexpr int kRowClasses = 6;
 
 // Fine-degree sum per coarse row.
 template <typename O>
@@ -196,14 +203,103 @@ __global__ void __launch_bounds__(kThreads) segment_warp_kernel(i64 rows, const 
     if (lane == 0) row_len[c] = __popc(heads);
 }
 
-// Rows with 33..seg_smem_capacity entries: block per row, radix sort in
-// shared memory.
+// Rows with 33..kWarpSegCap entries: one warp per row, LSD radix sort with
+// 8-bit digits in the warp's slice of shared memory (stable: equal digits
+// keep their order through __match_any_sync ranks), then the runs of equal
+// targets are summed 32 at a time with a carry between chunks.
+template <typename W>
+__global__ void __launch_bounds__(kThreads) segment_warp_radix_kernel(i64 rows, const i32* __restrict__ list,
+                                                                      const i64* __restrict__ temp_off, u32 sentinel,
+                                                                      int key_bits, u32* tgt, W* wt, i64* row_len) {
+    extern __shared__ unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    W* vbase = reinterpret_cast<W*>(smem_raw) + warp * 2 * kWarpSegCap;
+    u32* kbase = reinterpret_cast<u32*>(reinterpret_cast<W*>(smem_raw) + kWarps * 2 * kWarpSegCap) +
+                 warp * (2 * kWarpSegCap + kRadix);
+    W* v0 = vbase;
+    W* v1 = vbase + kWarpSegCap;
+    u32* k0 = kbase;
+    u32* k1 = kbase + kWarpSegCap;
+    u32* hist = kbase + 2 * kWarpSegCap;
+    const i64 r = static_cast<i64>(blockIdx.x) * kWarps + warp;
+    if (r >= rows) return;
+    const i32 c = list[r];
+    const i64 s = temp_off[c];
+    const int len = static_cast<int>(temp_off[c + 1] - s);
+    for (int i = lane; i < len; i += 32) { k0[i] = tgt[s + i]; v0[i] = wt[s + i]; }
+    __syncwarp();
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        for (int d = lane; d < kRadix; d += 32) hist[d] = 0;
+        __syncwarp();
+        for (int i = lane; i < len; i += 32) atomicAdd(&hist[(k0[i] >> shift) & (kRadix - 1)], 1u);
+        __syncwarp();
+        // exclusive scan of the 256 digit counts, 8 per lane
+        u32 cnt[kRadix / 32];
+        u32 tot = 0;
+#pragma unroll
+        for (int j = 0; j < kRadix / 32; ++j) { cnt[j] = hist[lane * (kRadix / 32) + j]; tot += cnt[j]; }
+        u32 ex = warp_inclusive_sum(tot) - tot;
+#pragma unroll
+        for (int j = 0; j < kRadix / 32; ++j) { hist[lane * (kRadix / 32) + j] = ex; ex += cnt[j]; }
+        __syncwarp();
+        for (int base = 0; base < len; base += 32) {
+            const int i = base + lane;
+            const bool valid = i < len;
+            const u32 key = valid ? k0[i] : 0u;
+            const W val = valid ? v0[i] : W(0);
+            const u32 dg = valid ? (key >> shift) & (kRadix - 1) : static_cast<u32>(kRadix);
+            const unsigned peers = __match_any_sync(0xffffffffu, dg);
+            const int leader = __ffs(peers) - 1;
+            u32 b = (valid && lane == leader) ? hist[dg] : 0u;
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (valid) {
+                const u32 pos = b + __popc(peers & lanemask_lt());
+                k1[pos] = key;
+                v1[pos] = val;
+            }
+            __syncwarp();
+            if (valid && lane == leader) hist[dg] = b + __popc(peers);
+            __syncwarp();
+        }
+        u32* tk = k0; k0 = k1; k1 = tk;
+        W* tv = v0; v0 = v1; v1 = tv;
+    }
+    // runs of the sorted segment; the sentinel (internal edges) sorts last
+    int u = 0;
+    u32 carry_key = 0xffffffffu;
+    W carry = 0;
+    for (int base = 0; base < len; base += 32) {
+        const int i = base + lane;
+        const bool valid = i < len;
+        const u32 key = valid ? k0[i] : sentinel;
+        W sum = warp_run_sum(valid ? v0[i] : W(0), key);
+        if (key == carry_key) sum += carry;
+        const u32 prev = __shfl_up_sync(0xffffffffu, key, 1);
+        u32 next = __shfl_down_sync(0xffffffffu, key, 1);
+        if (lane == 31) next = i + 1 < len ? k0[i + 1] : sentinel;   // first key of the next chunk
+        const bool real = valid && key != sentinel;
+        const bool head = real && (lane == 0 ? key != carry_key : prev != key);
+        const bool end = real && (i + 1 == len || next != key);
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        if (end) {
+            const int idx = u + __popc(heads & (lanemask_lt() | (1u << lane))) - 1;
+            tgt[s + idx] = key;
+            wt[s + idx] = sum;
+        }
+        u += __popc(heads);
+        carry_key = __shfl_sync(0xffffffffu, key, 31);
+        carry = __shfl_sync(0xffffffffu, sum, 31);
+    }
+    if (lane == 0) row_len[c] = u;
+}
+
+// Rows with kWarpSegCap+1..seg_smem_capacity entries: block per row, radix
+// sort in a shared-memory buffer of `cap` entries (the class's bound).
 template <typename W>
 __global__ void __launch_bounds__(kThreads) segment_smem_kernel(i64 rows, const i32* __restrict__ list,
                                                                 const i64* __restrict__ temp_off, u32 sentinel,
-                                                                int key_bits, u32* tgt, W* wt, i64* row_len) {
+                                                                int key_bits, int cap, u32* tgt, W* wt, i64* row_len) {
     extern __shared__ unsigned char smem_raw[];
-    constexpr int cap = seg_smem_capacity<W>();
     W* w0 = reinterpret_cast<W*>(smem_raw);
     W* w1 = w0 + cap;
     u32* k0 = reinterpret_cast<u32*>(w1 + cap);
@@ -246,24 +342,23 @@ __global__ void __launch_bounds__(kThreads) segment_global_kernel(i64 rows, cons
     if (threadIdx.x == 0) row_len[c] = u;
 }
 
-// Row-size classes: 0 empty, 1 <= 32, 2 <= smem_cap, 3 larger.
-// Classifies coarse rows by their number of scattered entries.  counts[0..3]
-// receive the rows per class, counts[4..7] the entries per class.
+// Classifies coarse rows by their number of scattered entries: counts[c]
+// receives the rows of class c, counts[kRowClasses + c] their entries.
 __global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u64* keys, i32* vals, u64* counts) {
-    __shared__ unsigned long long local[8];
-    if (threadIdx.x < 8) local[threadIdx.x] = 0;
+    __shared__ unsigned long long local[2 * kRowClasses];
+    if (threadIdx.x < 2 * kRowClasses) local[threadIdx.x] = 0;
     __syncthreads();
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c < rows) {
         const i64 l = temp_off[c + 1] - temp_off[c];
-        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= smem_cap ? 2 : 3;
+        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kWarpSegCap ? 2 : l <= kMidSegCap ? 3 : l <= smem_cap ? 4 : 5;
         keys[c] = static_cast<u64>(k);
         vals[c] = static_cast<i32>(c);
         atomicAdd(&local[k], 1ull);
-        atomicAdd(&local[4 + k], static_cast<unsigned long long>(l));
+        atomicAdd(&local[kRowClasses + k], static_cast<unsigned long long>(l));
     }
     __syncthreads();
-    if (threadIdx.x < 8 && local[threadIdx.x])
+    if (threadIdx.x < 2 * kRowClasses && local[threadIdx.x])
         atomicAdd(reinterpret_cast<unsigned long long*>(&counts[threadIdx.x]), local[threadIdx.x]);
 }
 

@@ -146,12 +146,13 @@ struct Log {
 struct Trace {
     bool on = std::getenv("GP_TRACE") != nullptr;
     std::chrono::steady_clock::time_point last = std::chrono::steady_clock::now();
-    void mark(Device& d, const char* what, long long a = -1) {
+    void mark(Device& d, const char* what, long long a = -1, long long b = -1) {
         if (!on) return;
         d.sync();
         const auto now = std::chrono::steady_clock::now();
         std::fprintf(stderr, "trace %-28s %8.3f ms", what, std::chrono::duration<double, std::milli>(now - last).count());
         if (a >= 0) std::fprintf(stderr, " (%lld)", a);
+        if (b >= 0) std::fprintf(stderr, " (%lld)", b);
         std::fprintf(stderr, "\n");
         last = std::chrono::steady_clock::now();
     }
@@ -573,35 +574,53 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     // row classes
     Buf<u64> rk(d, static_cast<size_t>(coarse_n)), rk_alt(d, static_cast<size_t>(coarse_n));
     Buf<i32> rl(d, static_cast<size_t>(coarse_n)), rl_alt(d, static_cast<size_t>(coarse_n));
-    Buf<u64> rc(d, 8);
+    Buf<u64> rc(d, 2 * kRowClasses);
     rc.zero(d);
     launch(d, "row_class_kernel", row_class_kernel, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n,
            temp_off.get(), static_cast<i64>(seg_smem_capacity<W>()), rk.get(), rl.get(), rc.get());
     GP_LAUNCH();
     radix_sort<u64, i32>(d, rk.get(), rl.get(), rk_alt.get(), rl_alt.get(), coarse_n, 0, 8);
-    u64 rcnt[8];
-    fetch(d, rcnt, rc.get(), 8);
+    u64 rcnt[2 * kRowClasses];
+    fetch(d, rcnt, rc.get(), 2 * kRowClasses);
+    const u64* rent = rcnt + kRowClasses;   // entries per class
+    i64 cstart[kRowClasses + 1] = {0};
+    for (int k = 0; k < kRowClasses; ++k) cstart[k + 1] = cstart[k] + static_cast<i64>(rcnt[k]);
     // segment kernels read and write each scattered entry once (target + weight)
-    d.prof_bytes("segment_warp_kernel", 2.0 * static_cast<double>(rcnt[5]) * (4 + sizeof(W)));
-    d.prof_bytes("segment_smem_kernel", 2.0 * static_cast<double>(rcnt[6]) * (4 + sizeof(W)));
-    d.prof_bytes("segment_global_kernel", 2.0 * static_cast<double>(rcnt[7]) * (4 + sizeof(W)));
-    const i64 c1 = rcnt[0], c2 = c1 + rcnt[1], c3 = c2 + rcnt[2];
+    auto seg_bytes = [&](int k) { return 2.0 * static_cast<double>(rent[k]) * (4 + sizeof(W)); };
+    d.prof_bytes("segment_warp_kernel", seg_bytes(1));
+    d.prof_bytes("segment_warp_radix_kernel", seg_bytes(2));
+    d.prof_bytes("segment_smem_kernel", seg_bytes(3) + seg_bytes(4));
+    d.prof_bytes("segment_global_kernel", seg_bytes(5));
     Buf<i64> row_len(d, static_cast<size_t>(coarse_n) + 1);
     row_len.zero(d);
     const int key_bits = std::max(1, bit_width_u64(static_cast<u64>(coarse_n)));
     if (rcnt[1])
-        launch(d, "segment_warp_kernel", segment_warp_kernel<W>, blocks_for(static_cast<i64>(rcnt[1]) * 32, kThreads), kThreads, 0, 
-            rcnt[1], rl.get() + c1, temp_off.get(), sentinel, tgt.get(), wt.get(), row_len.get());
+        launch(d, "segment_warp_kernel", segment_warp_kernel<W>, blocks_for(static_cast<i64>(rcnt[1]) * 32, kThreads),
+               kThreads, 0, rcnt[1], rl.get() + cstart[1], temp_off.get(), sentinel, tgt.get(), wt.get(),
+               row_len.get());
     if (rcnt[2]) {
-        const size_t smem = 2 * static_cast<size_t>(seg_smem_capacity<W>()) * (sizeof(u32) + sizeof(W));
-        GP_CUDA(cudaFuncSetAttribute(segment_smem_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const size_t smem = static_cast<size_t>(kWarps) * (2 * kWarpSegCap * sizeof(W) +
+                                                          (2 * kWarpSegCap + kRadix) * sizeof(u32));
+        GP_CUDA(cudaFuncSetAttribute(segment_warp_radix_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-        launch(d, "segment_smem_kernel", segment_smem_kernel<W>, static_cast<int>(rcnt[2]), kThreads, smem, 
-            rcnt[2], rl.get() + c2, temp_off.get(), sentinel, key_bits, tgt.get(), wt.get(), row_len.get());
+        launch(d, "segment_warp_radix_kernel", segment_warp_radix_kernel<W>,
+               blocks_for(static_cast<i64>(rcnt[2]) * 32, kThreads), kThreads, smem, rcnt[2], rl.get() + cstart[2],
+               temp_off.get(), sentinel, key_bits, tgt.get(), wt.get(), row_len.get());
+    }
+    for (int k = 3; k <= 4; ++k) {
+        if (!rcnt[k]) continue;
+        const int cap = k == 3 ? kMidSegCap : seg_smem_capacity<W>();
+        const size_t smem = 2 * static_cast<size_t>(cap) * (sizeof(u32) + sizeof(W));
+        GP_CUDA(cudaFuncSetAttribute(segment_smem_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(2 * static_cast<size_t>(seg_smem_capacity<W>()) *
+                                                      (sizeof(u32) + sizeof(W)))));
+        launch(d, "segment_smem_kernel", segment_smem_kernel<W>, static_cast<int>(rcnt[k]), kThreads, smem, rcnt[k],
+               rl.get() + cstart[k], temp_off.get(), sentinel, key_bits, cap, tgt.get(), wt.get(), row_len.get());
     }
     GP_LAUNCH();
-    if (rcnt[3]) {
-        const i64 big = rcnt[3];
+    const i64 c3 = cstart[5];
+    if (rcnt[5]) {
+        const i64 big = rcnt[5];
         Buf<i64> alt_off(d, static_cast<size_t>(big) + 1);
         exclusive_scan<i64>(d, BigRowLen{rl.get() + c3, temp_off.get(), big}, alt_off.get(), big + 1,
                             scal.get());
@@ -609,12 +628,12 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
         fetch(d, &alt_total, scal.get(), 1);
         Buf<u32> ak(d, static_cast<size_t>(alt_total));
         Buf<W> aw(d, static_cast<size_t>(alt_total));
-        launch(d, "segment_global_kernel", segment_global_kernel<W>, static_cast<int>(big), kThreads, 0, 
-            big, rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, key_bits, tgt.get(), wt.get(), ak.get(),
-            aw.get(), row_len.get());
+        launch(d, "segment_global_kernel", segment_global_kernel<W>, static_cast<int>(big), kThreads, 0,
+               big, rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, key_bits, tgt.get(), wt.get(), ak.get(),
+               aw.get(), row_len.get());
         GP_LAUNCH();
     }
-    trace().mark(d, "contract.segments", rcnt[3]);
+    trace().mark(d, "contract.segments", rcnt[5]);
     out.n = coarse_n;
     out.off = Buf<O>(d, static_cast<size_t>(coarse_n) + 1);
     exclusive_scan<O>(d, RowLenToO<O>{row_len.get()}, out.off.get(), coarse_n + 1, reinterpret_cast<O*>(scal.get() + 1));
@@ -628,8 +647,8 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
         d.prof_bytes("copy_rows_kernel", static_cast<double>(coarse_n) * (sizeof(O) + 8) + 2.0 * out.m * (4 + sizeof(W)));
         launch(d, "copy_rows_kernel", copy_rows_kernel<O, W>, blocks_for(((coarse_n + 31) / 32) * 32, kThreads),
                kThreads, 0, coarse_n, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
-        if (rcnt[3])
-            launch(d, "copy_big_rows_kernel", copy_big_rows_kernel<O, W>, static_cast<int>(rcnt[3]), kThreads, 0,
+        if (rcnt[5])
+            launch(d, "copy_big_rows_kernel", copy_big_rows_kernel<O, W>, static_cast<int>(rcnt[5]), kThreads, 0,
                    rl.get() + c3, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
         GP_LAUNCH();
     }
@@ -975,16 +994,19 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
                    0, hubs.chunk.get(), nbr, ew, labels, k, cache);
         }
     };
-    // Applies the listed movers.  When their edges outnumber m/8, updating the
-    // affinity cache edge by edge (two random atomics per edge) costs more
-    // than rebuilding it with one streaming pass, and the cut is then
-    // recounted exactly instead of being updated by the per-edge deltas; both
-    // routes give the same cache and the same cut.
+    // Applies the listed movers.  When the LP movers' edges outnumber m/8,
+    // updating the affinity cache edge by edge (two random atomics per edge)
+    // costs more than rebuilding it with one streaming pass, and the cut is
+    // then recounted exactly instead of being updated by the per-edge deltas;
+    // both routes give the same cache and the same cut.  (Rebalance moves
+    // stay edge by edge: measured, the rebuild plus recount does not pay
+    // there.)
     auto finish_apply = [&](bool lp) -> i64 {
         RefineCounters c0;
         fetch(d, &c0, ctr, 1);
         if (c0.movers == 0) return 0;
         const bool rebuild = lp && c0.mover_degree > g.m / 8;
+        trace().mark(d, lp ? "refine.select_lp" : "refine.select_balance", n);
         if (!rebuild) {
             // per mover: offsets, label and target; per mover edge: neighbour,
             // weight, the neighbour's label and two read-modify-writes of the cache
@@ -1001,6 +1023,7 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, c0.movers), kThreads, 0, w.movers.get(), ctr, labels,
                w.targets.get(), vw, pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
         if (rebuild) build_cache();
+        trace().mark(d, rebuild ? "refine.rebuild" : "refine.apply", c0.movers, c0.mover_degree);
         GP_CUDA(cudaMemcpyAsync(&stats_dev.get()->c, ctr, sizeof(RefineCounters), cudaMemcpyDeviceToDevice, d.stream));
         GP_CUDA(cudaMemcpyAsync(stats_dev.get()->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
         Stats h;
@@ -1068,8 +1091,9 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
-            launch(d, "select_destinations_kernel", select_destinations_kernel<W>, blocks_for(n, kThreads), kThreads, 0, 
-                n, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(), w.movers.get(), ctr);
+            launch(d, "select_destinations_kernel", select_destinations_kernel<O, W>, blocks_for(n, kThreads), kThreads,
+                   0, n, off, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(),
+                   w.movers.get(), ctr);
             GP_LAUNCH();
             const i64 moved = finish_apply(false);
             if (!moved) return false;

@@ -64,13 +64,13 @@ __device__ __forceinline__ int rows_per_warp(i64 count, i64 warps) {
 }
 
 // Inclusive sum over runs of equal, non-decreasing `key` across the warp.
-template <typename T>
-__device__ __forceinline__ T warp_run_sum(T v, int key) {
+template <typename T, typename K>
+__device__ __forceinline__ T warp_run_sum(T v, K key) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const T o = __shfl_up_sync(0xffffffffu, v, d);
-        const int ok = __shfl_up_sync(0xffffffffu, key, d);
+        const K ok = __shfl_up_sync(0xffffffffu, key, d);
         if (lane >= d && ok == key) v += o;
     }
     return v;

@@ -379,11 +379,13 @@ __global__ void select_sources_kernel(i64 n, i32* bucket, u64* rank, const u64* 
     if (!deterministic) rank[v] = atomic_add_u64(&counts[d], static_cast<u64>(weight_at(vw, v)));
 }
 
-// balance_select_destinations (src/refine_incremental.cuh:219-232)
-template <typename W>
-__global__ void select_destinations_kernel(i64 n, const i32* bucket, const u64* rank, const u64* offsets,
-                                           const u64* pw, u64 cap, const W* vw, unsigned char* flags, i32* movers,
-                                           RefineCounters* ctr) {
+// balance_select_destinations (src/refine_incremental.cuh:219-232); the
+// movers' degrees (hub rows excluded) are summed for the apply's choice
+// between edge-by-edge updates and a cache rebuild.
+template <typename O, typename W>
+__global__ void select_destinations_kernel(i64 n, const O* off, const i32* bucket, const u64* rank,
+                                           const u64* offsets, const u64* pw, u64 cap, const W* vw,
+                                           unsigned char* flags, i32* movers, RefineCounters* ctr) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (v >= n) return;
     const int b = bucket[v];
@@ -394,6 +396,9 @@ __global__ void select_destinations_kernel(i64 n, const i32* bucket, const u64* 
         flags[v] = 1;
         const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
         movers[slot] = static_cast<i32>(v);
+        const i64 deg = static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]);
+        if (deg <= kHubDegree)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree), static_cast<unsigned long long>(deg));
     }
 }
 
