@@ -7,8 +7,9 @@
 // 2. every segment is sorted by target and its runs of equal targets summed:
 //    a warp bitonic sort in registers for segments of <= 32 entries, a warp
 //    radix sort in the warp's shared memory for <= 256, a block radix sort in
-//    shared memory sized to the segment class for <= 4096, and a block radix
-//    sort through global scratch for larger (hub) segments;
+//    shared memory sized to the segment class for <= 4096, and, for larger
+//    segments, a block that ranks the targets through a shared-memory bitmap
+//    of the coarse id range instead of sorting;
 // 3. row lengths are scanned into the coarse offsets and the unique entries
 //    copied out.
 //
@@ -318,28 +319,96 @@ __global__ void __launch_bounds__(kThreads) segment_smem_kernel(i64 rows, const 
     if (threadIdx.x == 0) row_len[c] = u;
 }
 
-// Larger rows: block per row, radix sort ping-ponging through global scratch
-// (alt buffers at alt_off[r]).
+// Rows above seg_smem_capacity entries: block per row, no sort.  The row's
+// distinct targets are marked in a shared-memory bitmap over a window of the
+// coarse id range; a target's output position is then the number of marked
+// ids below it (a popcount prefix over 8-word groups), so the unique
+// (target, weight) pairs land in ascending target order while the weights
+// are summed by atomics.  Windows of kBitmapWindow ids are processed in
+// ascending order, each with two passes over the row's entries.  Output goes
+// to the row's alternate buffer (alt_off), which has room for all entries.
+constexpr int kBitmapWindow = 1 << 19;                 // ids per window (64 KB of bits)
+constexpr int kBitmapWords = kBitmapWindow / 32;
+constexpr int kBitmapGroup = 8;                        // words per prefix entry
+constexpr int kBitmapGroups = kBitmapWords / kBitmapGroup;
+
 template <typename W>
-__global__ void __launch_bounds__(kThreads) segment_global_kernel(i64 rows, const i32* __restrict__ list,
-                                                                  const i64* __restrict__ temp_off,
-                                                                  const i64* __restrict__ alt_off, u32 sentinel,
-                                                                  int key_bits, u32* tgt, W* wt, u32* alt_k, W* alt_w,
-                                                                  i64* row_len) {
-    __shared__ RankShared rank_sh;
-    __shared__ RunShared<W> run_sh;
+__global__ void __launch_bounds__(kThreads) segment_bitmap_kernel(
+    i64 rows, const i32* __restrict__ list, const i64* __restrict__ temp_off, const i64* __restrict__ alt_off,
+    u32 sentinel, i64 id_count, const u32* __restrict__ tgt, const W* __restrict__ wt, u32* alt_k, W* alt_w,
+    i64* row_len) {
+    extern __shared__ unsigned char smem_raw[];
+    u32* bits = reinterpret_cast<u32*>(smem_raw);
+    u32* gpre = bits + kBitmapWords;
+    __shared__ u32 scan_sh[kWarps + 1];
     const i64 r = blockIdx.x;
     if (r >= rows) return;
     const i32 c = list[r];
     const i64 s = temp_off[c];
     const i64 len = temp_off[c + 1] - s;
-    u32* ak = alt_k + alt_off[r];
-    W* aw = alt_w + alt_off[r];
-    block_radix_sort_segment(tgt + s, wt + s, ak, aw, len, 0, key_bits, rank_sh);
-    // runs are reduced out of the sorted data into the alt buffer, then copied back
-    const i64 u = block_reduce_runs(tgt + s, wt + s, len, sentinel, ak, aw, run_sh);
-    for (i64 i = threadIdx.x; i < u; i += kThreads) { tgt[s + i] = ak[i]; wt[s + i] = aw[i]; }
-    if (threadIdx.x == 0) row_len[c] = u;
+    u32* out_k = alt_k + alt_off[r];
+    W* out_w = alt_w + alt_off[r];
+    i64 unique = 0;
+    for (i64 lo = 0; lo < id_count; lo += kBitmapWindow) {
+        const i64 hi = lo + kBitmapWindow < id_count ? lo + kBitmapWindow : id_count;
+        const int words = static_cast<int>((hi - lo + 31) >> 5);
+        const int groups = (words + kBitmapGroup - 1) / kBitmapGroup;
+        for (int i = threadIdx.x; i < groups * kBitmapGroup; i += kThreads) bits[i] = 0;
+        __syncthreads();
+        for (i64 i = threadIdx.x; i < len; i += kThreads) {
+            const u32 t = tgt[s + i];
+            if (t != sentinel && t >= lo && t < hi) {
+                const u32 x = static_cast<u32>(t - lo);
+                atomicOr(&bits[x >> 5], 1u << (x & 31));
+            }
+        }
+        __syncthreads();
+        // exclusive prefix of the groups' popcounts
+        constexpr int kPer = kBitmapGroups / kThreads;   // groups per thread
+        u32 cnt[kPer];
+        u32 mine = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int g = threadIdx.x * kPer + j;
+            u32 pc = 0;
+            if (g < groups) {
+#pragma unroll
+                for (int q = 0; q < kBitmapGroup; ++q) pc += __popc(bits[g * kBitmapGroup + q]);
+            }
+            cnt[j] = pc;
+            mine += pc;
+        }
+        u32 total = 0;
+        u32 run = block_exclusive_sum<u32>(mine, scan_sh, &total);
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int g = threadIdx.x * kPer + j;
+            if (g < groups) gpre[g] = run;
+            run += cnt[j];
+        }
+        for (i64 i = threadIdx.x; i < total; i += kThreads) out_w[unique + i] = W(0);
+        __syncthreads();
+        for (i64 i = threadIdx.x; i < len; i += kThreads) {
+            const u32 t = tgt[s + i];
+            if (t != sentinel && t >= lo && t < hi) {
+                const u32 x = static_cast<u32>(t - lo);
+                const int w = static_cast<int>(x >> 5);
+                const int g = w / kBitmapGroup;
+                u32 rank = gpre[g] + __popc(bits[w] & ((1u << (x & 31)) - 1u));
+                for (int q = g * kBitmapGroup; q < w; ++q) rank += __popc(bits[q]);
+                const i64 pos = unique + rank;
+                out_k[pos] = t;
+                if constexpr (sizeof(W) == 8)
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&out_w[pos]),
+                              static_cast<unsigned long long>(wt[s + i]));
+                else
+                    atomicAdd(reinterpret_cast<unsigned*>(&out_w[pos]), static_cast<unsigned>(wt[s + i]));
+            }
+        }
+        unique += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) row_len[c] = unique;
 }
 
 // Classifies coarse rows by their number of scattered entries: counts[c]
@@ -381,8 +450,8 @@ struct BigRowLen {
 
 // Copy each row's unique entries from its segment to the final CSR; a warp
 // per 32 rows in a virtual position space as in scatter_edges_kernel.  Rows
-// whose segment exceeded the shared-memory capacity are copied by
-// copy_big_rows_kernel.
+// whose segment exceeded the shared-memory capacity are copied from their
+// alternate buffers by copy_big_rows_kernel.
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64* __restrict__ temp_off,
                                                              const O* __restrict__ coff, const u32* __restrict__ tgt,
@@ -420,15 +489,16 @@ __global__ void __launch_bounds__(kThreads) copy_rows_kernel(i64 rows, const i64
 
 template <typename O, typename W>
 __global__ void __launch_bounds__(kThreads) copy_big_rows_kernel(const i32* __restrict__ list,
-                                                                 const i64* __restrict__ temp_off,
+                                                                 const i64* __restrict__ alt_off,
                                                                  const O* __restrict__ coff,
-                                                                 const u32* __restrict__ tgt, const W* __restrict__ wt,
+                                                                 const u32* __restrict__ alt_k,
+                                                                 const W* __restrict__ alt_w,
                                                                  i32* __restrict__ nbr, W* __restrict__ ew) {
     const i32 r = list[blockIdx.x];
-    const i64 ds = coff[r], len = static_cast<i64>(coff[r + 1]) - ds, src = temp_off[r];
+    const i64 ds = coff[r], len = static_cast<i64>(coff[r + 1]) - ds, src = alt_off[blockIdx.x];
     for (i64 i = threadIdx.x; i < len; i += kThreads) {
-        nbr[ds + i] = static_cast<i32>(tgt[src + i]);
-        ew[ds + i] = wt[src + i];
+        nbr[ds + i] = static_cast<i32>(alt_k[src + i]);
+        ew[ds + i] = alt_w[src + i];
     }
 }
 

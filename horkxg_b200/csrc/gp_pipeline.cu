@@ -590,7 +590,7 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     d.prof_bytes("segment_warp_kernel", seg_bytes(1));
     d.prof_bytes("segment_warp_radix_kernel", seg_bytes(2));
     d.prof_bytes("segment_smem_kernel", seg_bytes(3) + seg_bytes(4));
-    d.prof_bytes("segment_global_kernel", seg_bytes(5));
+    d.prof_bytes("segment_bitmap_kernel", seg_bytes(5));
     Buf<i64> row_len(d, static_cast<size_t>(coarse_n) + 1);
     row_len.zero(d);
     const int key_bits = std::max(1, bit_width_u64(static_cast<u64>(coarse_n)));
@@ -619,17 +619,23 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     }
     GP_LAUNCH();
     const i64 c3 = cstart[5];
+    Buf<i64> alt_off;
+    Buf<u32> ak;
+    Buf<W> aw;
     if (rcnt[5]) {
         const i64 big = rcnt[5];
-        Buf<i64> alt_off(d, static_cast<size_t>(big) + 1);
+        alt_off = Buf<i64>(d, static_cast<size_t>(big) + 1);
         exclusive_scan<i64>(d, BigRowLen{rl.get() + c3, temp_off.get(), big}, alt_off.get(), big + 1,
                             scal.get());
         i64 alt_total = 0;
         fetch(d, &alt_total, scal.get(), 1);
-        Buf<u32> ak(d, static_cast<size_t>(alt_total));
-        Buf<W> aw(d, static_cast<size_t>(alt_total));
-        launch(d, "segment_global_kernel", segment_global_kernel<W>, static_cast<int>(big), kThreads, 0,
-               big, rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, key_bits, tgt.get(), wt.get(), ak.get(),
+        ak = Buf<u32>(d, static_cast<size_t>(alt_total));
+        aw = Buf<W>(d, static_cast<size_t>(alt_total));
+        const size_t smem = (static_cast<size_t>(kBitmapWords) + kBitmapGroups) * sizeof(u32);
+        GP_CUDA(cudaFuncSetAttribute(segment_bitmap_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        launch(d, "segment_bitmap_kernel", segment_bitmap_kernel<W>, static_cast<int>(big), kThreads, smem, big,
+               rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, coarse_n, tgt.get(), wt.get(), ak.get(),
                aw.get(), row_len.get());
         GP_LAUNCH();
     }
@@ -649,7 +655,7 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
                kThreads, 0, coarse_n, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
         if (rcnt[5])
             launch(d, "copy_big_rows_kernel", copy_big_rows_kernel<O, W>, static_cast<int>(rcnt[5]), kThreads, 0,
-                   rl.get() + c3, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
+                   rl.get() + c3, alt_off.get(), out.off.get(), ak.get(), aw.get(), out.nbr.get(), out.ew.get());
         GP_LAUNCH();
     }
     out.vw = std::move(cvw);
@@ -1091,9 +1097,9 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
-            launch(d, "select_destinations_kernel", select_destinations_kernel<O, W>, blocks_for(n, kThreads), kThreads,
-                   0, n, off, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(),
-                   w.movers.get(), ctr);
+            launch(d, "select_destinations_kernel", select_destinations_kernel<W>, blocks_for(n, kThreads), kThreads,
+                   0, n, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(), w.movers.get(),
+                   ctr);
             GP_LAUNCH();
             const i64 moved = finish_apply(false);
             if (!moved) return false;

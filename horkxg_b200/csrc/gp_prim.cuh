@@ -55,6 +55,20 @@ __device__ __forceinline__ void warp_edge_walk(i64 begin, i64 deg, F&& f) {
     }
 }
 
+// Appends the lanes whose `pred` holds to a list of length *counter with one
+// atomic per warp; returns each appending lane's slot.  All 32 lanes call it.
+__device__ __forceinline__ u64 warp_append(bool pred, u64* counter) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return 0;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader)
+        base = atomicAdd(reinterpret_cast<unsigned long long*>(counter), static_cast<unsigned long long>(__popc(m)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return static_cast<u64>(base) + __popc(m & lanemask_lt());
+}
+
 // Rows a warp takes at once in a warp_edge_walk loop over `count` rows: up to
 // 32 when there are many, down to one per warp when there are few (a walk
 // over fewer rows than warps would leave most warps idle).

@@ -120,28 +120,35 @@ __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i3
                                     double filter, unsigned char* locks, i32* targets, i64* gains, PropRec* props,
                                     i32* list, RefineCounters* ctr) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    targets[v] = -1;
-    gains[v] = INT64_MIN;
-    const i32 s = labels[v];
-    props[v] = {s, -1, INT64_MIN};
-    if (locks[v]) { locks[v] = 0; return; }
-    const C* row = cache + v * k;
-    u64 best = 0;
-    int target = -1;
-    for (int p = 0; p < k; ++p) {
-        const u64 c = static_cast<u64>(row[p]);
-        if (p != s && c > best) { best = c; target = p; }
-    }
-    const u64 current = static_cast<u64>(row[s]);
-    if (target >= 0 && (best >= current || current - best < static_cast<u64>(filter * static_cast<double>(current)))) {
-        const i64 g = best >= current ? static_cast<i64>(best - current) : -static_cast<i64>(current - best);
+    bool propose = false;
+    if (v < n) {
+        i32 target = -1;
+        i64 g = INT64_MIN;
+        const i32 s = labels[v];
+        if (locks[v]) {
+            locks[v] = 0;
+        } else {
+            const C* row = cache + v * k;
+            u64 best = 0;
+            int t = -1;
+            for (int p = 0; p < k; ++p) {
+                const u64 c = static_cast<u64>(row[p]);
+                if (p != s && c > best) { best = c; t = p; }
+            }
+            const u64 current = static_cast<u64>(row[s]);
+            if (t >= 0 &&
+                (best >= current || current - best < static_cast<u64>(filter * static_cast<double>(current)))) {
+                g = best >= current ? static_cast<i64>(best - current) : -static_cast<i64>(current - best);
+                target = t;
+                propose = true;
+            }
+        }
         targets[v] = target;
         gains[v] = g;
         props[v] = {s, target, g};
-        const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->proposers), 1ULL);
-        list[slot] = static_cast<i32>(v);
     }
+    const u64 slot = warp_append(propose, reinterpret_cast<u64*>(&ctr->proposers));
+    if (propose) list[slot] = static_cast<i32>(v);
 }
 
 // incremental_priority_filter (src/refine_incremental.cuh:48-67); movers are
@@ -189,12 +196,16 @@ __global__ void __launch_bounds__(kThreads) priority_filter_kernel(
             if ((lane == 31 || next != owner) && run != 0) corr_sh[warp][owner] += run;
             __syncwarp();
         });
-        if (has && !hub && me.gain + corr_sh[warp][lane] >= 0) {
+        const bool move = has && !hub && me.gain + corr_sh[warp][lane] >= 0;
+        const u64 slot = warp_append(move, reinterpret_cast<u64*>(&ctr->movers));
+        if (move) {
             flags[v] = 1;
-            const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
             movers[slot] = v;
-            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree), static_cast<unsigned long long>(deg));
         }
+        const i64 moved_degree = warp_sum(move ? deg : i64{0});
+        if (lane == 0 && moved_degree)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree),
+                      static_cast<unsigned long long>(moved_degree));
         __syncwarp();
     }
 }
@@ -379,26 +390,25 @@ __global__ void select_sources_kernel(i64 n, i32* bucket, u64* rank, const u64* 
     if (!deterministic) rank[v] = atomic_add_u64(&counts[d], static_cast<u64>(weight_at(vw, v)));
 }
 
-// balance_select_destinations (src/refine_incremental.cuh:219-232); the
-// movers' degrees (hub rows excluded) are summed for the apply's choice
-// between edge-by-edge updates and a cache rebuild.
-template <typename O, typename W>
-__global__ void select_destinations_kernel(i64 n, const O* off, const i32* bucket, const u64* rank,
-                                           const u64* offsets, const u64* pw, u64 cap, const W* vw,
-                                           unsigned char* flags, i32* movers, RefineCounters* ctr) {
+// balance_select_destinations (src/refine_incremental.cuh:219-232).
+template <typename W>
+__global__ void select_destinations_kernel(i64 n, const i32* bucket, const u64* rank, const u64* offsets,
+                                           const u64* pw, u64 cap, const W* vw, unsigned char* flags, i32* movers,
+                                           RefineCounters* ctr) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const int b = bucket[v];
-    if (b < 0) return;
-    const u64 before = offsets[b] + rank[v];
-    const u64 slack = cap - pw[b / kBalWidth];
-    if (before <= slack && static_cast<u64>(weight_at(vw, v)) <= slack - before) {
+    bool move = false;
+    if (v < n) {
+        const int b = bucket[v];
+        if (b >= 0) {
+            const u64 before = offsets[b] + rank[v];
+            const u64 slack = cap - pw[b / kBalWidth];
+            move = before <= slack && static_cast<u64>(weight_at(vw, v)) <= slack - before;
+        }
+    }
+    const u64 slot = warp_append(move, reinterpret_cast<u64*>(&ctr->movers));
+    if (move) {
         flags[v] = 1;
-        const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->movers), 1ULL);
         movers[slot] = static_cast<i32>(v);
-        const i64 deg = static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]);
-        if (deg <= kHubDegree)
-            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->mover_degree), static_cast<unsigned long long>(deg));
     }
 }
 
