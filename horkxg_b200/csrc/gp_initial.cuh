@@ -67,38 +67,52 @@ struct NormShared {
 
 // Every block computes every task's (mean, scale) from the per-position
 // contributions in the same order: deterministic and identical everywhere.
+// The tasks are reduced side by side: `wpt` warps per task, each warp over a
+// lane-strided slice with an xor-shuffle tree, then one thread per task adds
+// its warps' partials in warp order.
 __device__ void compute_norms(int tasks, const InitTask* task, const Moments* contrib, NormShared& sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t = 0; t < tasks; ++t) {
-        const i32 b = task[t].begin, c = task[t].count;
+    int wpt = kWarps;
+    while (wpt > 1 && tasks * wpt > kWarps) wpt >>= 1;
+    const int per_round = kWarps / wpt;
+    for (int t0 = 0; t0 < tasks; t0 += per_round) {
+        const int t = t0 + warp / wpt;
+        const int part = warp % wpt;
         float m = 0.f, s = 0.f, q = 0.f;
-        for (i32 i = threadIdx.x; i < c; i += kThreads) {
-            const Moments x = contrib[b + i];
-            m += x.mass; s += x.sum; q += x.squares;
-        }
+        if (t < tasks) {
+            const i32 b = task[t].begin, c = task[t].count;
+            for (i32 i = part * 32 + lane; i < c; i += wpt * 32) {
+                const Moments x = contrib[b + i];
+                m += x.mass; s += x.sum; q += x.squares;
+            }
 #pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            m += __shfl_xor_sync(0xffffffffu, m, o);
-            s += __shfl_xor_sync(0xffffffffu, s, o);
-            q += __shfl_xor_sync(0xffffffffu, q, o);
+            for (int o = 16; o; o >>= 1) {
+                m += __shfl_xor_sync(0xffffffffu, m, o);
+                s += __shfl_xor_sync(0xffffffffu, s, o);
+                q += __shfl_xor_sync(0xffffffffu, q, o);
+            }
         }
         if (lane == 0) { sh.red[0][warp] = m; sh.red[1][warp] = s; sh.red[2][warp] = q; }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < per_round && t0 + static_cast<int>(threadIdx.x) < tasks) {
             float M = 0.f, S = 0.f, Q = 0.f;
-            for (int w = 0; w < kWarps; ++w) { M += sh.red[0][w]; S += sh.red[1][w]; Q += sh.red[2][w]; }
+            for (int w = threadIdx.x * wpt; w < (static_cast<int>(threadIdx.x) + 1) * wpt; ++w) {
+                M += sh.red[0][w]; S += sh.red[1][w]; Q += sh.red[2][w];
+            }
             const float mean = S / M;
             const float var = fmaxf(0.f, Q / M - mean * mean);
-            sh.mean[t] = mean;
-            sh.scale[t] = var > 1e-30f ? 1.0f / sqrtf(var) : 1.0f;
+            sh.mean[t0 + threadIdx.x] = mean;
+            sh.scale[t0 + threadIdx.x] = var > 1e-30f ? 1.0f / sqrtf(var) : 1.0f;
         }
         __syncthreads();
     }
 }
 
 // Rows longer than this are reduced by a whole block (fixed tree), shorter
-// ones by one warp, so the step time is not set by the densest row.
-constexpr i64 kHeavyRow = 512;
+// ones by one warp, so the step time is not set by the densest row.  Coarsest
+// levels of power-law graphs are nearly complete (degrees in the thousands),
+// and a block reduction per row costs more than a warp walking the row.
+constexpr i64 kHeavyRow = 4096;
 
 // Sum over a row range of f(e) restricted to the group, with four
 // independent loads in flight per lane.  `stride` is the number of lanes
