@@ -29,9 +29,11 @@ __host__ __device__ constexpr int seg_smem_capacity() { return 4096; }
 constexpr int kWarpSegCap = 256;    // warp radix sort
 constexpr int kMidSegCap = 1024;    // block radix sort with a 1024-entry buffer
 
+constexpr i64 kGiantSeg = 1 << 16;  // above: rows spread over many blocks
+
 // Row-size classes: 0 empty, 1 <= 32, 2 <= kWarpSegCap, 3 <= kMidSegCap,
-// 4 <= seg_smem_capacity, 5 larger.
-constexpr int kRowClasses = 6;
+// 4 <= seg_smem_capacity, 5 <= kGiantSeg, 6 larger.
+constexpr int kRowClasses = 7;
 
 // Fine-degree sum per coarse row.
 template <typename O>
@@ -411,6 +413,111 @@ __global__ void __launch_bounds__(kThreads) segment_bitmap_kernel(
     if (threadIdx.x == 0) row_len[c] = unique;
 }
 
+// Giant rows (more than kGiantSeg entries; the rows of hub clusters) would
+// leave one block working long after the rest of the GPU is idle.  Their
+// entries are cut into kGiantChunk-entry chunks spread over all SMs: one
+// pass marks the targets in a global bitmap per row (coarse id range), a
+// block per row scans the words' popcounts into per-8-word-group prefixes,
+// and a second pass over the chunks writes each (target, weight) at its rank
+// in the row's alternate buffer, summing weights with atomics.
+constexpr i64 kGiantChunk = 8192;
+
+struct SegChunk {
+    i32 row;        // index among the giant rows
+    i32 pad;
+    i64 begin, end; // entry range in the scattered arrays
+};
+
+struct GiantChunkCount {
+    const i32* list;
+    const i64* temp_off;
+    i64 count;
+    __device__ i64 operator()(i64 i) const {
+        if (i >= count) return 0;
+        const i32 c = list[i];
+        return (temp_off[c + 1] - temp_off[c] + kGiantChunk - 1) / kGiantChunk;
+    }
+};
+
+__global__ void giant_chunks_kernel(i64 giants, const i32* __restrict__ list, const i64* __restrict__ temp_off,
+                                    const i64* __restrict__ chunk_off, SegChunk* chunks) {
+    const i64 g = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= giants) return;
+    const i32 c = list[g];
+    const i64 s = temp_off[c], e = temp_off[c + 1];
+    for (i64 q = chunk_off[g]; q < chunk_off[g + 1]; ++q) {
+        const i64 b = s + (q - chunk_off[g]) * kGiantChunk;
+        chunks[q] = {static_cast<i32>(g), 0, b, b + kGiantChunk < e ? b + kGiantChunk : e};
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) giant_mark_kernel(const SegChunk* __restrict__ chunks,
+                                                              const u32* __restrict__ tgt, u32 sentinel,
+                                                              i64 words_per_row, u32* gbits) {
+    const SegChunk ch = chunks[blockIdx.x];
+    u32* bits = gbits + static_cast<i64>(ch.row) * words_per_row;
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const u32 t = tgt[e];
+        if (t != sentinel) atomicOr(&bits[t >> 5], 1u << (t & 31));
+    }
+}
+
+// Block per giant row: gpre[g] = marked ids in the row's words before group g
+// (kBitmapGroup words per group); row_len = the row's marked ids.
+__global__ void __launch_bounds__(kThreads) giant_scan_kernel(const i32* __restrict__ list, i64 words_per_row,
+                                                              const u32* __restrict__ gbits, u32* gpre,
+                                                              i64* row_len) {
+    __shared__ u32 scan_sh[kWarps + 1];
+    const i64 groups = (words_per_row + kBitmapGroup - 1) / kBitmapGroup;
+    const u32* bits = gbits + static_cast<i64>(blockIdx.x) * words_per_row;
+    u32* pre = gpre + static_cast<i64>(blockIdx.x) * groups;
+    const i64 per = (groups + kThreads - 1) / kThreads;
+    const i64 g0 = static_cast<i64>(threadIdx.x) * per;
+    const i64 g1 = g0 + per < groups ? g0 + per : groups;
+    auto group_count = [&](i64 g) {
+        u32 pc = 0;
+        for (i64 w = g * kBitmapGroup; w < (g + 1) * kBitmapGroup && w < words_per_row; ++w) pc += __popc(bits[w]);
+        return pc;
+    };
+    u32 mine = 0;
+    for (i64 g = g0; g < g1; ++g) mine += group_count(g);
+    u32 total = 0;
+    u32 run = block_exclusive_sum<u32>(mine, scan_sh, &total);
+    for (i64 g = g0; g < g1; ++g) {
+        pre[g] = run;
+        run += group_count(g);
+    }
+    if (threadIdx.x == 0) row_len[list[blockIdx.x]] = total;
+}
+
+template <typename W>
+__global__ void __launch_bounds__(kThreads) giant_place_kernel(const SegChunk* __restrict__ chunks,
+                                                               const u32* __restrict__ tgt, const W* __restrict__ wt,
+                                                               u32 sentinel, i64 words_per_row,
+                                                               const u32* __restrict__ gbits,
+                                                               const u32* __restrict__ gpre,
+                                                               const i64* __restrict__ alt_off, u32* alt_k, W* alt_w) {
+    const SegChunk ch = chunks[blockIdx.x];
+    const i64 groups = (words_per_row + kBitmapGroup - 1) / kBitmapGroup;
+    const u32* bits = gbits + static_cast<i64>(ch.row) * words_per_row;
+    const u32* pre = gpre + static_cast<i64>(ch.row) * groups;
+    u32* out_k = alt_k + alt_off[ch.row];
+    W* out_w = alt_w + alt_off[ch.row];
+    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+        const u32 t = tgt[e];
+        if (t == sentinel) continue;
+        const i64 w = t >> 5;
+        const i64 g = w / kBitmapGroup;
+        u32 rank = pre[g] + __popc(bits[w] & ((1u << (t & 31)) - 1u));
+        for (i64 q = g * kBitmapGroup; q < w; ++q) rank += __popc(bits[q]);
+        out_k[rank] = t;
+        if constexpr (sizeof(W) == 8)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&out_w[rank]), static_cast<unsigned long long>(wt[e]));
+        else
+            atomicAdd(reinterpret_cast<unsigned*>(&out_w[rank]), static_cast<unsigned>(wt[e]));
+    }
+}
+
 // Classifies coarse rows by their number of scattered entries: counts[c]
 // receives the rows of class c, counts[kRowClasses + c] their entries.
 __global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u64* keys, i32* vals, u64* counts) {
@@ -420,7 +527,8 @@ __global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u6
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c < rows) {
         const i64 l = temp_off[c + 1] - temp_off[c];
-        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kWarpSegCap ? 2 : l <= kMidSegCap ? 3 : l <= smem_cap ? 4 : 5;
+        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kWarpSegCap ? 2 : l <= kMidSegCap ? 3 : l <= smem_cap ? 4
+                    : l <= kGiantSeg ? 5 : 6;
         keys[c] = static_cast<u64>(k);
         vals[c] = static_cast<i32>(c);
         atomicAdd(&local[k], 1ull);

@@ -591,6 +591,7 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     d.prof_bytes("segment_warp_radix_kernel", seg_bytes(2));
     d.prof_bytes("segment_smem_kernel", seg_bytes(3) + seg_bytes(4));
     d.prof_bytes("segment_bitmap_kernel", seg_bytes(5));
+    d.prof_bytes("giant_place_kernel", seg_bytes(6));
     Buf<i64> row_len(d, static_cast<size_t>(coarse_n) + 1);
     row_len.zero(d);
     const int key_bits = std::max(1, bit_width_u64(static_cast<u64>(coarse_n)));
@@ -618,12 +619,14 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
                rl.get() + cstart[k], temp_off.get(), sentinel, key_bits, cap, tgt.get(), wt.get(), row_len.get());
     }
     GP_LAUNCH();
+    // rows above seg_smem_capacity (classes 5 and 6, contiguous in the class
+    // order) are written to alternate buffers
     const i64 c3 = cstart[5];
+    const i64 big = static_cast<i64>(rcnt[5] + rcnt[6]);
     Buf<i64> alt_off;
     Buf<u32> ak;
     Buf<W> aw;
-    if (rcnt[5]) {
-        const i64 big = rcnt[5];
+    if (big) {
         alt_off = Buf<i64>(d, static_cast<size_t>(big) + 1);
         exclusive_scan<i64>(d, BigRowLen{rl.get() + c3, temp_off.get(), big}, alt_off.get(), big + 1,
                             scal.get());
@@ -631,15 +634,45 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
         fetch(d, &alt_total, scal.get(), 1);
         ak = Buf<u32>(d, static_cast<size_t>(alt_total));
         aw = Buf<W>(d, static_cast<size_t>(alt_total));
+    }
+    if (rcnt[5]) {
         const size_t smem = (static_cast<size_t>(kBitmapWords) + kBitmapGroups) * sizeof(u32);
         GP_CUDA(cudaFuncSetAttribute(segment_bitmap_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-        launch(d, "segment_bitmap_kernel", segment_bitmap_kernel<W>, static_cast<int>(big), kThreads, smem, big,
-               rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, coarse_n, tgt.get(), wt.get(), ak.get(),
-               aw.get(), row_len.get());
+        launch(d, "segment_bitmap_kernel", segment_bitmap_kernel<W>, static_cast<int>(rcnt[5]), kThreads, smem,
+               static_cast<i64>(rcnt[5]), rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, coarse_n, tgt.get(),
+               wt.get(), ak.get(), aw.get(), row_len.get());
         GP_LAUNCH();
     }
-    trace().mark(d, "contract.segments", rcnt[5]);
+    if (rcnt[6]) {
+        const i64 giants = static_cast<i64>(rcnt[6]);
+        const i32* glist = rl.get() + cstart[6];
+        const i64* galt = alt_off.get() + rcnt[5];
+        Buf<i64> chunk_off(d, static_cast<size_t>(giants) + 1);
+        exclusive_scan<i64>(d, GiantChunkCount{glist, temp_off.get(), giants}, chunk_off.get(), giants + 1,
+                            scal.get());
+        i64 gbase = 0, chunks_total = 0;
+        fetch(d, &chunks_total, scal.get(), 1);
+        fetch(d, &gbase, galt, 1);
+        Buf<SegChunk> chunks(d, static_cast<size_t>(chunks_total));
+        launch(d, "giant_chunks_kernel", giant_chunks_kernel, blocks_for(giants, kThreads), kThreads, 0, giants,
+               glist, temp_off.get(), chunk_off.get(), chunks.get());
+        const i64 wpr = (coarse_n + 31) / 32;
+        const i64 groups = (wpr + kBitmapGroup - 1) / kBitmapGroup;
+        Buf<u32> gbits(d, static_cast<size_t>(giants * wpr));
+        Buf<u32> gpre(d, static_cast<size_t>(giants * groups));
+        gbits.zero(d);
+        GP_CUDA(cudaMemsetAsync(aw.get() + gbase, 0,
+                                static_cast<size_t>(static_cast<i64>(ak.size()) - gbase) * sizeof(W), d.stream));
+        launch(d, "giant_mark_kernel", giant_mark_kernel, static_cast<int>(chunks_total), kThreads, 0, chunks.get(),
+               tgt.get(), sentinel, wpr, gbits.get());
+        launch(d, "giant_scan_kernel", giant_scan_kernel, static_cast<int>(giants), kThreads, 0, glist, wpr,
+               gbits.get(), gpre.get(), row_len.get());
+        launch(d, "giant_place_kernel", giant_place_kernel<W>, static_cast<int>(chunks_total), kThreads, 0,
+               chunks.get(), tgt.get(), wt.get(), sentinel, wpr, gbits.get(), gpre.get(), galt, ak.get(), aw.get());
+        GP_LAUNCH();
+    }
+    trace().mark(d, "contract.segments", static_cast<long long>(rcnt[5]), static_cast<long long>(rcnt[6]));
     out.n = coarse_n;
     out.off = Buf<O>(d, static_cast<size_t>(coarse_n) + 1);
     exclusive_scan<O>(d, RowLenToO<O>{row_len.get()}, out.off.get(), coarse_n + 1, reinterpret_cast<O*>(scal.get() + 1));
@@ -653,8 +686,8 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
         d.prof_bytes("copy_rows_kernel", static_cast<double>(coarse_n) * (sizeof(O) + 8) + 2.0 * out.m * (4 + sizeof(W)));
         launch(d, "copy_rows_kernel", copy_rows_kernel<O, W>, blocks_for(((coarse_n + 31) / 32) * 32, kThreads),
                kThreads, 0, coarse_n, temp_off.get(), out.off.get(), tgt.get(), wt.get(), out.nbr.get(), out.ew.get());
-        if (rcnt[5])
-            launch(d, "copy_big_rows_kernel", copy_big_rows_kernel<O, W>, static_cast<int>(rcnt[5]), kThreads, 0,
+        if (big)
+            launch(d, "copy_big_rows_kernel", copy_big_rows_kernel<O, W>, static_cast<int>(big), kThreads, 0,
                    rl.get() + c3, alt_off.get(), out.off.get(), ak.get(), aw.get(), out.nbr.get(), out.ew.get());
         GP_LAUNCH();
     }

@@ -108,7 +108,7 @@ def test_identity_and_empty_contraction(ctx):
     assert list(coff) == [0] * 5 and len(cnbr) == 0
 
 
-@pytest.mark.parametrize("name,groups", [("rmat14", 700), ("rmat16", 40), ("grid2d_256", 9000)])
+@pytest.mark.parametrize("name,groups", [("rmat14", 700), ("rmat16", 40), ("rmat16", 20), ("grid2d_256", 9000)])
 def test_contraction_random_maps(ctx, name, groups):
     off, idx, g = file_graph(name)
     rng = np.random.default_rng(groups)
@@ -117,6 +117,26 @@ def test_contraction_random_maps(ctx, name, groups):
     coff, cnbr, cew, cvw = ctx.contract(g, mapping, groups)
     o = O.contract(O.Graph(off, idx), mapping, groups)
     assert np.array_equal(coff, o.off) and np.array_equal(cnbr, o.nbr) and np.array_equal(cew, o.ew)
+
+
+def test_contraction_large_id_range(ctx):
+    """More coarse ids than one shared-memory bitmap window holds, with rows
+    of every size class: identity for most vertices, the rest folded into
+    2000 rows of a few thousand entries and 8 rows above the giant-row bound."""
+    off, idx, g = file_graph("rmat20")
+    n = len(off) - 1
+    keep = 600_000
+    mapping = np.arange(n, dtype=np.int64)
+    rest = np.arange(keep, n)
+    mapping[keep:] = np.where(rest % 5 == 0, keep + rest % 8, keep + 8 + rest % 2000)
+    mapping = mapping.astype(np.int32)
+    groups = keep + 2008
+    coff, cnbr, cew, cvw = ctx.contract(g, mapping, groups)
+    o = O.contract(O.Graph(off, idx), mapping, groups)
+    assert np.array_equal(coff, o.off) and np.array_equal(cnbr, o.nbr) and np.array_equal(cew, o.ew)
+    assert np.array_equal(cvw, o.vw)
+    sizes = np.diff(o.off)
+    assert sizes.max() > 4096
 
 
 # --- FP32 diffusion vs FP64 oracle (src/initial_partition_gpu.cu:81-142)
