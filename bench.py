@@ -48,6 +48,7 @@ WORKLOADS = {
     # profiling-size case of the default workload (same generator, 1/4 the vertices)
     "rmat20_k32": ("rmat20", 32, "standard", "RMAT scale 20 ef16 (0.57,0.19,0.19) seed 1, symmetrised, k=32, standard"),
     "grid3d_320_k32": ("grid3d_320", 32, "big", "3D 7-point grid 320^3, k=32, big"),
+    "grid3d_320_k8": ("grid3d_320", 8, "big", "3D 7-point grid 320^3, k=8, big"),
 }
 
 
@@ -428,6 +429,12 @@ def run_ours(args, rank, world, local, dist):
     torch.cuda.synchronize()
     e_elapsed = dist.max(e_start.elapsed_time(e_stop) * 1e-3)
 
+    # final cut over seeds 0..4 (untimed), for the cut-quality comparison
+    # with the reference's median over the same seeds
+    seed_cuts = []
+    for sd in range(args.cut_seeds):
+        seed_cuts.append(int(ctx.partition_desc(ddesc, d_lab.data_ptr(), hb.default_options(parts=parts, seed=sd)).cut))
+
     # per-kernel profile of one more step (outside the timed region)
     ctx.profile(True)
     ctx.partition_desc(ddesc, d_lab.data_ptr(), opts)
@@ -449,6 +456,7 @@ def run_ours(args, rank, world, local, dist):
                        "parts": parts, "width": width, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (0.5 GB CSR), no flush"},
             "cut": int(statistics.median(cuts)), "max_part_weight": int(loads.max()), "capacity": int(cap),
+            "cut_seeds": seed_cuts, "cut_median_seeds": int(statistics.median(seed_cuts)) if seed_cuts else None,
             "algorithm_seconds_median": statistics.median(r.algorithm_seconds for r in reports),
             "stage_seconds": {"coarsen": reports[-1].coarsen_seconds, "initial": reports[-1].initial_seconds,
                               "uncoarsen": reports[-1].uncoarsen_seconds, "free": reports[-1].free_seconds},
@@ -487,9 +495,9 @@ def run_reference(args, rank, world, local, dist):
     out = Path("/tmp") / f"gp_ref_{args.workload}.part"
     algo, walls, cuts = [], [], []
 
-    def once():
+    def once(seed=0):
         t0 = time.perf_counter()
-        text = subprocess.run([str(exe), str(indptr), str(indices), str(parts), str(out), "1.03", "0"],
+        text = subprocess.run([str(exe), str(indptr), str(indices), str(parts), str(out), "1.03", str(seed)],
                               capture_output=True, text=True, check=True, env=env).stdout
         wall = time.perf_counter() - t0
         a = float(re.findall(r"algorithm_total_seconds=([0-9.e+-]+)", text)[-1])
@@ -499,11 +507,14 @@ def run_reference(args, rank, world, local, dist):
     for _ in range(args.warmup):
         once()
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            a, w, c = once()
+        for i in range(args.steps):
+            a, w, c = once(i % 5)   # seeds 0..4 in turn (the timing does not depend on the seed)
             algo.append(a)
             walls.append(w)
             cuts.append(c)
+    seed_cuts = cuts[:5]
+    for sd in range(len(seed_cuts), min(5, args.cut_seeds)):
+        seed_cuts.append(once(sd)[2])
     total = sum(algo)
     value = m * args.steps / total
     return {
@@ -513,6 +524,7 @@ def run_reference(args, rank, world, local, dist):
         "config": {"workload": desc, "graph": WORKLOADS[args.workload][0], "vertices": n, "edges": m,
                    "parts": parts, "width": width, "parallelism": "replicas1"},
         "cut": int(statistics.median(cuts)),
+        "cut_seeds": seed_cuts, "cut_median_seeds": int(statistics.median(seed_cuts)) if seed_cuts else None,
         "process_seconds_median": statistics.median(walls),
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 0, "kind": "reference",
@@ -535,6 +547,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the Poisson request stream (the serving workload is 60 s; 0 skips it)")
     ap.add_argument("--slots", type=int, default=8, help="server slots for the batched and serving workloads")
+    ap.add_argument("--cut-seeds", type=int, default=5, help="untimed partitions with seeds 0..N-1 for the cut median")
     args = ap.parse_args()
     rank, world, local = dist_env()
     dist = Dist(world)

@@ -942,7 +942,7 @@ u64 undirected_cut(Device& d, const DGraph<T>& g, const i32* labels, u64* scratc
 
 struct RefineWork {
     Buf<unsigned char> cache_raw;
-    Buf<i32> targets, list, movers, saved_labels, clist, clist_alt;
+    Buf<i32> targets, list, movers, saved_labels, clist, clist_alt, cand;
     Buf<i64> gains, pos;
     Buf<PropRec> props;
     Buf<unsigned char> locks, flags;
@@ -954,7 +954,7 @@ struct RefineWork {
         const size_t s = static_cast<size_t>(n) + 1;
         cache_raw.ensure(d, cache_bytes);
         targets.ensure(d, s); list.ensure(d, s); movers.ensure(d, s); saved_labels.ensure(d, s);
-        clist.ensure(d, s); clist_alt.ensure(d, s);
+        clist.ensure(d, s); clist_alt.ensure(d, s); cand.ensure(d, s);
         gains.ensure(d, s); pos.ensure(d, s); props.ensure(d, s);
         locks.ensure(d, s); flags.ensure(d, s);
         gpw.ensure(d, s); bucket.ensure(d, s);
@@ -1086,11 +1086,13 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         }
         return h.c.movers;
     };
+    i64 ncand = 0;   // rebalance candidates in w.cand (vertices of overloaded parts, ascending)
     auto deterministic_ranks = [&]() {
         // candidates in ascending vertex order, sorted by (bucket, gpw desc)
-        exclusive_scan<i64>(d, HasBucket{w.bucket.get()}, w.pos.get(), n, reinterpret_cast<i64*>(w.scratch.get() + 1));
-        launch(d, "compact_bucket_kernel", compact_bucket_kernel, blocks_for(n, kThreads), kThreads, 0, n, w.bucket.get(), w.pos.get(),
-                                                                                  w.clist.get());
+        exclusive_scan<i64>(d, HasBucket{w.bucket.get(), w.cand.get()}, w.pos.get(), ncand,
+                            reinterpret_cast<i64*>(w.scratch.get() + 1));
+        launch(d, "compact_bucket_kernel", compact_bucket_kernel, blocks_for(ncand, kThreads), kThreads, 0, ncand,
+               w.cand.get(), w.bucket.get(), w.pos.get(), w.clist.get());
         GP_LAUNCH();
         i64 count = 0;
         fetch(d, &count, reinterpret_cast<i64*>(w.scratch.get() + 1), 1);
@@ -1113,26 +1115,33 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         GP_LAUNCH();
     };
     auto rebalance = [&]() -> bool {
+        if (maximum() <= cap) return true;
+        exclusive_scan<i64>(d, InOverloaded{labels, pw, cap}, w.pos.get(), n,
+                            reinterpret_cast<i64*>(w.scratch.get() + 1));
+        launch(d, "compact_overloaded_kernel", compact_overloaded_kernel, blocks_for(n, kThreads), kThreads, 0, n,
+               labels, pw, cap, w.pos.get(), w.cand.get());
+        fetch(d, &ncand, reinterpret_cast<i64*>(w.scratch.get() + 1), 1);
+        const int cgrid = blocks_for(std::max<i64>(ncand, 1), kThreads);
         for (int it = 0; it < 2 * k + 4 && maximum() > cap; ++it) {
             ++st.admission_iterations;
             GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
             w.counts.zero(d);
-            launch(d, "rebalance_proposals_kernel", rebalance_proposals_kernel<C, W>, blocks_for(n, kThreads), kThreads, 0, 
-                n, cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(), w.gpw.get(),
-                w.bucket.get(), w.rank.get(), w.counts.get());
+            launch(d, "rebalance_proposals_kernel", rebalance_proposals_kernel<C, W>, cgrid, kThreads, 0, ncand,
+                   w.cand.get(), cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(),
+                   w.gpw.get(), w.bucket.get(), w.rank.get(), w.counts.get());
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
             w.counts.zero(d);
-            launch(d, "select_sources_kernel", select_sources_kernel<W>, blocks_for(n, kThreads), kThreads, 0, 
-                n, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, w.targets.get(), vw, deterministic ? 1 : 0,
-                w.counts.get());
+            launch(d, "select_sources_kernel", select_sources_kernel<W>, cgrid, kThreads, 0, ncand, w.cand.get(),
+                   w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, w.targets.get(), vw, deterministic ? 1 : 0,
+                   w.counts.get());
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
-            launch(d, "select_destinations_kernel", select_destinations_kernel<W>, blocks_for(n, kThreads), kThreads,
-                   0, n, w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(), w.movers.get(),
-                   ctr);
+            launch(d, "select_destinations_kernel", select_destinations_kernel<W>, cgrid, kThreads, 0, ncand,
+                   w.cand.get(), w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(),
+                   w.movers.get(), ctr);
             GP_LAUNCH();
             const i64 moved = finish_apply(false);
             if (!moved) return false;
@@ -1182,20 +1191,18 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     return st;
 }
 
+// The affinity cache can hold 32-bit sums when the level's total directed
+// edge weight fits in 32 bits (whatever the graph width): no row sum can
+// exceed it.
 template <typename T>
 bool narrow_cache(const DGraph<T>& g, Device& d) {
-    if constexpr (sizeof(typename T::W) == 8) {
-        (void)g; (void)d;
-        return false;
-    } else {
-        Buf<u64> s(d, 1);
-        s.zero(d);
-        launch(d, "sat_sum_kernel", sat_sum_kernel<typename T::W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), s.get());
-        GP_LAUNCH();
-        u64 total = 0;
-        fetch(d, &total, s.get(), 1);
-        return total <= 0xffffffffULL;
-    }
+    Buf<u64> s(d, 1);
+    s.zero(d);
+    launch(d, "sat_sum_kernel", sat_sum_kernel<typename T::W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), s.get());
+    GP_LAUNCH();
+    u64 total = 0;
+    fetch(d, &total, s.get(), 1);
+    return total <= 0xffffffffULL;
 }
 
 template <typename T>

@@ -79,6 +79,39 @@ __device__ __forceinline__ u64 group_sum(unsigned peers, u64 w) {
     }
 }
 
+// One vertex's k cache entries into registers, with 16-byte loads when the
+// row is 16-byte aligned (k a multiple of 4 for 32-bit entries, of 2 for
+// 64-bit entries); entries past k are left untouched.
+template <typename C>
+__device__ __forceinline__ void load_row(const C* row, int k, C (&vals)[32]) {
+    if constexpr (sizeof(C) == 4) {
+        if ((k & 3) == 0) {
+            const uint4* r4 = reinterpret_cast<const uint4*>(row);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (4 * q < k) {
+                    const uint4 x = r4[q];
+                    vals[4 * q] = x.x; vals[4 * q + 1] = x.y; vals[4 * q + 2] = x.z; vals[4 * q + 3] = x.w;
+                }
+            return;
+        }
+    } else {
+        if ((k & 1) == 0) {
+            const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(row);
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                if (2 * q < k) {
+                    const ulonglong2 x = r2[q];
+                    vals[2 * q] = x.x; vals[2 * q + 1] = x.y;
+                }
+            return;
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 32; ++p)
+        if (p < k) vals[p] = row[p];
+}
+
 // incremental_build_affinity (src/refine_incremental.cuh:7-25), warp per
 // vertex.  Lanes holding the same part are grouped with __match_any_sync and
 // only the group leader adds to the warp's private row, so the row needs no
@@ -128,14 +161,17 @@ __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i3
         if (locks[v]) {
             locks[v] = 0;
         } else {
-            const C* row = cache + v * k;
-            u64 best = 0;
+            C vals[32];
+            load_row(cache + v * k, k, vals);
+            u64 best = 0, current = 0;
             int t = -1;
-            for (int p = 0; p < k; ++p) {
-                const u64 c = static_cast<u64>(row[p]);
-                if (p != s && c > best) { best = c; t = p; }
+#pragma unroll
+            for (int p = 0; p < 32; ++p) {
+                if (p >= k) break;
+                const u64 c = static_cast<u64>(vals[p]);
+                if (p == s) current = c;
+                else if (c > best) { best = c; t = p; }
             }
-            const u64 current = static_cast<u64>(row[s]);
             if (t >= 0 &&
                 (best >= current || current - best < static_cast<u64>(filter * static_cast<double>(current)))) {
                 g = best >= current ? static_cast<i64>(best - current) : -static_cast<i64>(current - best);
@@ -217,8 +253,8 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
     const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
     const i32* __restrict__ targets, const unsigned char* __restrict__ flags, int k, C* cache, RefineCounters* ctr) {
     // A warp takes up to 32 movers and walks their edges together (hub rows:
-    // chunked kernel).
-    __shared__ long long sh[kWarps + 1];
+    // chunked kernel).  The cut delta is summed per warp and added with one
+    // atomic per warp, so warps never wait for each other.
     const int lane = threadIdx.x & 31;
     const i64 count = ctr_in->movers;
     const i64 warps = static_cast<i64>(gridDim.x) * kWarps;
@@ -240,18 +276,18 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
             const i32 u = nbr[e];
             if (u == ov) return;
             const u64 w = static_cast<u64>(weight_at(ew, e));
+            const bool fu = flags[u] != 0;
+            const i32 lu = labels[u];
             cache_add(&cache[static_cast<i64>(u) * k + os], 0ULL - w);
             cache_add(&cache[static_cast<i64>(u) * k + ot], w);
-            const bool fu = flags[u] != 0;
             if (!fu || u > ov) {
-                const i32 lu = labels[u];
                 const i32 nn = fu ? targets[u] : lu;
                 gain += static_cast<long long>(w) * ((os != lu) - (ot != nn));
             }
         });
     }
-    gain = block_sum(gain, sh);
-    if (threadIdx.x == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));
+    gain = warp_sum(gain);
+    if (lane == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));
 }
 
 // incremental_commit (src/refine_incremental.cuh:97-109); also clears the
@@ -299,29 +335,65 @@ __device__ __forceinline__ int gain_bucket(double g, const BucketThresholds& th)
     return 25 + (lo - 23);
 }
 
+// Ranks of weighted items in per-key counters with one atomic per key and
+// warp: the lanes that share a key take consecutive ranges in lane order, as
+// if their atomicAdds had run back to back (the reference's ranks come from
+// plain atomicAdds in scheduling order, so any such order is one it can
+// produce).  All 32 lanes call it; key < 0 means no item.
+__device__ __forceinline__ u64 warp_rank_add(int key, u64 w, bool unit, u64* counts) {
+    const int lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const unsigned lower = peers & lanemask_lt();
+    u64 before = 0, total = 0;
+    if (unit) {
+        before = static_cast<u64>(__popc(lower));
+        total = static_cast<u64>(__popc(peers));
+    } else {
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            const u64 x = __shfl_sync(0xffffffffu, w, s);
+            if ((peers >> s) & 1u) {
+                total += x;
+                if (s < lane) before += x;
+            }
+        }
+    }
+    const int leader = __ffs(peers) - 1;
+    u64 base = 0;
+    if (key >= 0 && lane == leader) base = atomic_add_u64(&counts[key], total);
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + before;
+}
+
 // incremental_rebalance_proposals + balance_source_histogram
 // (src/refine_incremental.cuh:111-186).  Atomic mode ranks here; the
 // deterministic mode appends candidates (ascending vertex order is restored by
 // the scan-based compaction that follows).
+// One rebalance candidate: the destination with slack that it is best
+// connected to (ties: more slack), a zero-connection vertex spread over the
+// parts with slack by a hashed ticket; returns the vertex's bucket
+// (source part, gain-per-weight bucket, hashed section) or -1.
 template <typename C, typename W>
-__global__ void rebalance_proposals_kernel(i64 n, const C* __restrict__ cache, const i32* __restrict__ labels,
-                                           const W* __restrict__ vw, int k, const u64* __restrict__ pw, u64 cap,
-                                           BucketThresholds th, int deterministic, i32* targets, double* gpw,
-                                           i32* bucket, u64* rank, u64* counts) {
-    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (v >= n) return;
+__device__ __forceinline__ int rebalance_choice(i64 v, const C* __restrict__ cache, const i32* __restrict__ labels,
+                                                const W* __restrict__ vw, int k, const u64* spw, u64 cap,
+                                                const BucketThresholds& th, i32* targets, double* gpw, i32* bucket,
+                                                u64& w) {
     targets[v] = -1;
     bucket[v] = -1;
     const i32 s = labels[v];
-    if (pw[s] <= cap) return;
-    const u64 w = static_cast<u64>(weight_at(vw, v));
-    const C* row = cache + v * k;
+    if (spw[s] <= cap) return -1;
+    w = static_cast<u64>(weight_at(vw, v));
+    C vals[32];
+    load_row(cache + v * k, k, vals);
     int best = -1;
-    u64 best_conn = 0, best_slack = 0;
-    for (int p = 0; p < k; ++p) {
-        const u64 pp = pw[p];
-        if (p == s || pp >= cap || w > cap - pp) continue;
-        const u64 value = static_cast<u64>(row[p]);
+    u64 best_conn = 0, best_slack = 0, current = 0;
+#pragma unroll
+    for (int p = 0; p < 32; ++p) {
+        if (p >= k) break;
+        const u64 value = static_cast<u64>(vals[p]);
+        if (p == s) { current = value; continue; }
+        const u64 pp = spw[p];
+        if (pp >= cap || w > cap - pp) continue;
         const u64 slack = cap - pp;
         if (best < 0 || value > best_conn || (value == best_conn && slack > best_slack)) {
             best = p; best_conn = value; best_slack = slack;
@@ -330,29 +402,50 @@ __global__ void rebalance_proposals_kernel(i64 n, const C* __restrict__ cache, c
     if (best >= 0 && best_conn == 0) {
         u64 total_slack = 0;
         for (int p = 0; p < k; ++p) {
-            const u64 pp = pw[p];
+            const u64 pp = spw[p];
             if (p != s && pp < cap && w <= cap - pp)
                 total_slack = UINT64_MAX - total_slack < cap - pp ? UINT64_MAX : total_slack + cap - pp;
         }
         u64 ticket = static_cast<u64>(mix32(static_cast<u32>(v))) % total_slack;
         for (int p = 0; p < k; ++p) {
-            const u64 pp = pw[p];
+            const u64 pp = spw[p];
             if (p == s || pp >= cap || w > cap - pp) continue;
             const u64 slack = cap - pp;
             if (ticket < slack) { best = p; break; }
             ticket -= slack;
         }
     }
-    if (best < 0) return;
-    const u64 current = static_cast<u64>(row[s]);
+    if (best < 0) return -1;
     const double gain = best_conn >= current ? static_cast<double>(best_conn - current)
                                              : -static_cast<double>(current - best_conn);
     const double g = gain / static_cast<double>(w);
     targets[v] = best;
     gpw[v] = g;
-    const int b = s * kBalWidth + gain_bucket(g, th) * kBalSections + static_cast<int>(mix32(static_cast<u32>(v)) % kBalSections);
+    const int b = s * kBalWidth + gain_bucket(g, th) * kBalSections +
+                  static_cast<int>(mix32(static_cast<u32>(v)) % kBalSections);
     bucket[v] = b;
-    if (!deterministic) rank[v] = atomic_add_u64(&counts[b], w);
+    return b;
+}
+
+// Over the candidate list (vertices of overloaded parts); part weights are
+// staged in shared memory.
+template <typename C, typename W>
+__global__ void rebalance_proposals_kernel(i64 n, const i32* __restrict__ list, const C* __restrict__ cache,
+                                           const i32* __restrict__ labels, const W* __restrict__ vw, int k,
+                                           const u64* __restrict__ pw, u64 cap, BucketThresholds th,
+                                           int deterministic, i32* targets, double* gpw, i32* bucket, u64* rank,
+                                           u64* counts) {
+    __shared__ u64 spw[32];
+    if (threadIdx.x < 32) spw[threadIdx.x] = static_cast<int>(threadIdx.x) < k ? pw[threadIdx.x] : ~0ULL;
+    __syncthreads();
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const i64 v = i < n ? (list ? list[i] : i) : 0;
+    u64 w = 0;
+    const int b = i < n ? rebalance_choice(v, cache, labels, vw, k, spw, cap, th, targets, gpw, bucket, w) : -1;
+    if (!deterministic) {
+        const u64 r = warp_rank_add(b, w, vw == nullptr, counts);
+        if (b >= 0) rank[v] = r;
+    }
 }
 
 // balance_scan_buckets (src/refine_incremental.cuh:188-202): exclusive scan
@@ -379,25 +472,37 @@ __global__ void __launch_bounds__(kThreads) bucket_scan_kernel(const u64* counts
 
 // balance_select_sources (src/refine_incremental.cuh:204-217)
 template <typename W>
-__global__ void select_sources_kernel(i64 n, i32* bucket, u64* rank, const u64* offsets, const u64* pw, u64 cap,
-                                      const i32* targets, const W* vw, int deterministic, u64* counts) {
-    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (v >= n || bucket[v] < 0) return;
-    const int b = bucket[v], s = b / kBalWidth;
-    if (offsets[b] + rank[v] >= pw[s] - cap) { bucket[v] = -1; return; }
-    const int d = targets[v] * kBalWidth + b % kBalWidth;
-    bucket[v] = d;
-    if (!deterministic) rank[v] = atomic_add_u64(&counts[d], static_cast<u64>(weight_at(vw, v)));
+__global__ void select_sources_kernel(i64 n, const i32* __restrict__ list, i32* bucket, u64* rank, const u64* offsets,
+                                      const u64* pw, u64 cap, const i32* targets, const W* vw, int deterministic,
+                                      u64* counts) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const i64 v = i < n ? (list ? list[i] : i) : 0;
+    int d = -1;
+    if (i < n && bucket[v] >= 0) {
+        const int b = bucket[v], s = b / kBalWidth;
+        if (offsets[b] + rank[v] >= pw[s] - cap) {
+            bucket[v] = -1;
+        } else {
+            d = targets[v] * kBalWidth + b % kBalWidth;
+            bucket[v] = d;
+        }
+    }
+    if (!deterministic) {
+        const u64 r = warp_rank_add(d, i < n ? static_cast<u64>(weight_at(vw, v)) : 0, vw == nullptr, counts);
+        if (d >= 0) rank[v] = r;
+    }
 }
 
 // balance_select_destinations (src/refine_incremental.cuh:219-232).
 template <typename W>
-__global__ void select_destinations_kernel(i64 n, const i32* bucket, const u64* rank, const u64* offsets,
-                                           const u64* pw, u64 cap, const W* vw, unsigned char* flags, i32* movers,
-                                           RefineCounters* ctr) {
-    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+__global__ void select_destinations_kernel(i64 n, const i32* __restrict__ list, const i32* bucket, const u64* rank,
+                                           const u64* offsets, const u64* pw, u64 cap, const W* vw,
+                                           unsigned char* flags, i32* movers, RefineCounters* ctr) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     bool move = false;
-    if (v < n) {
+    i64 v = 0;
+    if (i < n) {
+        v = list ? list[i] : i;
         const int b = bucket[v];
         if (b >= 0) {
             const u64 before = offsets[b] + rank[v];
@@ -417,12 +522,31 @@ __global__ void select_destinations_kernel(i64 n, const i32* bucket, const u64* 
 // the bucket; counts = bucket totals.
 struct HasBucket {
     const i32* bucket;
-    __device__ i64 operator()(i64 i) const { return bucket[i] >= 0 ? 1 : 0; }
+    const i32* list;   // candidate vertices (ascending), or null for all
+    __device__ i64 operator()(i64 i) const { return bucket[list ? list[i] : i] >= 0 ? 1 : 0; }
 };
 
-__global__ void compact_bucket_kernel(i64 n, const i32* bucket, const i64* pos, i32* list) {
+__global__ void compact_bucket_kernel(i64 n, const i32* cand, const i32* bucket, const i64* pos, i32* list) {
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const i64 v = cand ? cand[i] : i;
+    if (bucket[v] >= 0) list[pos[i]] = static_cast<i32>(v);
+}
+
+// Vertices of the parts above capacity: the only rebalance candidates, and a
+// superset of them for the whole rebalance (destinations never exceed the
+// capacity, so no part becomes overloaded and vertices only leave).
+struct InOverloaded {
+    const i32* labels;
+    const u64* pw;
+    u64 cap;
+    __device__ i64 operator()(i64 v) const { return pw[labels[v]] > cap ? 1 : 0; }
+};
+
+__global__ void compact_overloaded_kernel(i64 n, const i32* labels, const u64* pw, u64 cap, const i64* pos,
+                                          i32* list) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (v < n && bucket[v] >= 0) list[pos[v]] = static_cast<i32>(v);
+    if (v < n && pw[labels[v]] > cap) list[pos[v]] = static_cast<i32>(v);
 }
 
 // mode 0: ~orderable(gpw) (desc); mode 1: bucket
