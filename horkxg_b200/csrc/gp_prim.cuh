@@ -335,11 +335,33 @@ struct U32ToI64 {
     __device__ i64 operator()(i64 i) const { return static_cast<i64>(a[i]); }
 };
 
+template <typename K, typename V>
+__device__ void block_radix_sort_segment(K* keys, V* vals, K* keys_alt, V* vals_alt, i64 count, int begin_bit,
+                                         int end_bit, RankShared& sh);
+
+// Whole sort of a small array by one block (all passes in one launch).
+template <typename K, typename V>
+__global__ void __launch_bounds__(kThreads) small_radix_sort_kernel(K* keys, V* vals, K* keys_alt, V* vals_alt, i64 n,
+                                                                    int begin_bit, int end_bit) {
+    __shared__ RankShared sh;
+    block_radix_sort_segment(keys, vals, keys_alt, vals_alt, n, begin_bit, end_bit, sh);
+}
+
+constexpr i64 kSmallSort = 8192;   // one-block sort up to this many keys
+
 // Sorts bits [begin_bit, end_bit) of the keys.  On return the sorted data is
 // in (keys, vals) (the routine copies back after an odd number of passes).
+// Small arrays are sorted by one block in one launch: on small graphs the
+// multi-launch passes cost more in launch latency than in work.
 template <typename K, typename V>
 void radix_sort(Device& d, K* keys, V* vals, K* keys_alt, V* vals_alt, i64 n, int begin_bit, int end_bit) {
     if (n <= 1 || begin_bit >= end_bit) return;
+    if (n <= kSmallSort) {
+        launch(d, "small_radix_sort_kernel", small_radix_sort_kernel<K, V>, 1, kThreads, 0, keys, vals, keys_alt,
+               vals_alt, n, begin_bit, end_bit);
+        GP_LAUNCH();
+        return;
+    }
     const int grid = static_cast<int>(std::min<i64>(std::max<i64>(1, (n + kSortTile - 1) / kSortTile),
                                                     static_cast<i64>(d.sms) * 4));
     Buf<u32> hist(d, static_cast<size_t>(kRadix) * grid);
