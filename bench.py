@@ -38,6 +38,8 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# one hardware work queue per server slot stream (read at CUDA context creation)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 WORKLOADS = {
     # name: (graph, parts, width, description)

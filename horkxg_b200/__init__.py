@@ -11,9 +11,17 @@ Loading fails loudly when the library is missing: there is no fallback.
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 
 import numpy as np
+
+# A server runs one CUDA stream per slot; with the driver's default of 8
+# hardware work queues, more than 8 streams share queues and their kernels
+# serialise behind each other.  The setting is read when the process creates
+# its CUDA context, so it only takes effect if this module is imported before
+# any CUDA work; an explicit setting is kept.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libgpart_b200.so"
@@ -65,7 +73,7 @@ class RefineStats(ctypes.Structure):
 EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_error", "gp_partition_capacity",
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
-           "gp_launch_count", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
+           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
            "gp_initial_partition_static", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
            "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
            "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
@@ -101,6 +109,9 @@ def lib() -> ctypes.CDLL:
         L.gp_cut.argtypes = [vp, P(GraphDesc), vp, i32, P(ctypes.c_uint64), vp]
         L.gp_launch_count.argtypes = [vp]
         L.gp_launch_count.restype = ctypes.c_uint64
+        L.gp_sync_count.argtypes = [vp]
+        L.gp_sync_count.restype = ctypes.c_uint64
+        L.gp_ctx_set_sync_mode.argtypes = [vp, i32]
         L.gp_ctx_stream.argtypes = [vp]
         L.gp_ctx_stream.restype = vp
         L.gp_profile_enable.argtypes = [vp, i32]
@@ -336,6 +347,10 @@ class Context:
     @property
     def launches(self) -> int:
         return int(lib().gp_launch_count(self._h))
+
+    @property
+    def syncs(self) -> int:
+        return int(lib().gp_sync_count(self._h))
 
     @property
     def stream(self) -> int:

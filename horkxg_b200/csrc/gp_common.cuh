@@ -146,7 +146,20 @@ struct Device {
         live.erase(it);
     }
     [[noreturn]] static void throw_oom(size_t bytes);
-    void sync() { GP_CUDA(cudaStreamSynchronize(stream)); }
+    u64 syncs = 0;     // host waits on the stream (round trips)
+    // Blocking waits put the host thread to sleep until the stream's work is
+    // done instead of spinning on a core (for processes with many contexts).
+    cudaEvent_t sync_event = nullptr;
+    bool blocking_sync = false;
+    void sync() {
+        ++syncs;
+        if (blocking_sync) {
+            GP_CUDA(cudaEventRecord(sync_event, stream));
+            GP_CUDA(cudaEventSynchronize(sync_event));
+        } else {
+            GP_CUDA(cudaStreamSynchronize(stream));
+        }
+    }
     // Read a device error word; throws on any set bit.
     void check_errors();
 

@@ -316,31 +316,50 @@ __global__ void hub_filter_finalize_kernel(i64 hubs, const i32* __restrict__ hub
               static_cast<unsigned long long>(static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v])));
 }
 
+// Cache and cut update of the hub rows among the movers.  Most applies (the
+// rebalance iterations) move no hub, so a launch of one block per chunk would
+// mostly schedule blocks that exit at once.  Instead a grid of at most a few
+// blocks per SM strides over the chunks: each block first tests the mover flag
+// of up to 256 of its chunks in parallel, then walks the flagged chunks one
+// after another with all its threads.
 template <typename W, typename C>
-__global__ void __launch_bounds__(kThreads) hub_apply_kernel(const Chunk* __restrict__ chunks,
+__global__ void __launch_bounds__(kThreads) hub_apply_kernel(i64 nchunks, const Chunk* __restrict__ chunks,
                                                              const i32* __restrict__ nbr, const W* __restrict__ ew,
                                                              const i32* __restrict__ labels,
                                                              const i32* __restrict__ targets,
                                                              const unsigned char* __restrict__ flags, int k,
                                                              C* cache, RefineCounters* ctr) {
     __shared__ long long sh[kWarps + 1];
-    const Chunk ch = chunks[blockIdx.x];
-    const i32 v = ch.v;
-    if (!flags[v]) return;
-    const i32 s = labels[v], t = targets[v];
+    __shared__ int todo[kThreads];
+    __shared__ int ntodo;
+    const i64 stride = gridDim.x;
     long long gain = 0;
-    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
-        const i32 u = nbr[e];
-        if (u == v) continue;
-        const u64 w = static_cast<u64>(weight_at(ew, e));
-        cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
-        cache_add(&cache[static_cast<i64>(u) * k + t], w);
-        const bool fu = flags[u] != 0;
-        if (!fu || u > v) {
-            const i32 lu = labels[u];
-            const i32 nn = fu ? targets[u] : lu;
-            gain += static_cast<long long>(w) * ((s != lu) - (t != nn));
+    for (i64 base = blockIdx.x; base < nchunks; base += stride * kThreads) {
+        if (threadIdx.x == 0) ntodo = 0;
+        __syncthreads();
+        const i64 mine = base + static_cast<i64>(threadIdx.x) * stride;
+        if (mine < nchunks && flags[chunks[mine].v]) todo[atomicAdd(&ntodo, 1)] = static_cast<int>(threadIdx.x);
+        __syncthreads();
+        const int count = ntodo;
+        for (int j = 0; j < count; ++j) {
+            const Chunk ch = chunks[base + static_cast<i64>(todo[j]) * stride];
+            const i32 v = ch.v;
+            const i32 s = labels[v], t = targets[v];
+            for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+                const i32 u = nbr[e];
+                if (u == v) continue;
+                const u64 w = static_cast<u64>(weight_at(ew, e));
+                cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
+                cache_add(&cache[static_cast<i64>(u) * k + t], w);
+                const bool fu = flags[u] != 0;
+                if (!fu || u > v) {
+                    const i32 lu = labels[u];
+                    const i32 nn = fu ? targets[u] : lu;
+                    gain += static_cast<long long>(w) * ((s != lu) - (t != nn));
+                }
+            }
         }
+        __syncthreads();
     }
     gain = block_sum(gain, sh);
     if (threadIdx.x == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta),

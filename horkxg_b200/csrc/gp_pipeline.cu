@@ -1039,27 +1039,35 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     // then recounted exactly instead of being updated by the per-edge deltas;
     // both routes give the same cache and the same cut.  (Rebalance moves
     // stay edge by edge: measured, the rebuild plus recount does not pay
-    // there.)
+    // there.)  The kernels read the mover count from the device, so a
+    // rebalance apply needs no round trip before its launch: its grids are
+    // sized for the candidate count, an upper bound of its movers.
+    i64 ncand = 0;   // rebalance candidates in w.cand (vertices of overloaded parts, ascending)
     auto finish_apply = [&](bool lp) -> i64 {
-        RefineCounters c0;
-        fetch(d, &c0, ctr, 1);
-        if (c0.movers == 0) return 0;
+        RefineCounters c0{};
+        const bool read_first = lp || d.prof || trace().on;
+        if (read_first) {
+            fetch(d, &c0, ctr, 1);
+            if (c0.movers == 0) return 0;
+        }
+        const i64 bound = read_first ? c0.movers : ncand;
         const bool rebuild = lp && c0.mover_degree > g.m / 8;
         trace().mark(d, lp ? "refine.select_lp" : "refine.select_balance", n);
         if (!rebuild) {
-            // per mover: offsets, label and target; per mover edge: neighbour,
-            // weight, the neighbour's label and two read-modify-writes of the cache
-            d.prof_bytes("apply_cache_cut_kernel",
-                         static_cast<double>(c0.movers) * (2 * sizeof(O) + 4 + 4 + 4) +
-                             static_cast<double>(c0.mover_degree) * (4 + 4 + (ew ? sizeof(W) : 0) + 4 * sizeof(C)));
-            launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, c0.movers * 32),
+            // w.list (the LP proposers) is free once the movers are selected:
+            // it takes the movers of degree above kSplitDegree
+            launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, bound * 32),
                    kThreads, 0, w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache,
-                   ctr);
+                   ctr, w.list.get());
+            launch(d, "apply_big_rows_kernel", apply_big_rows_kernel<O, W, C>,
+                   static_cast<int>(std::min<i64>(std::max<i64>(bound, 1), static_cast<i64>(d.sms) * 4)), kThreads, 0,
+                   w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
             if (hubs.count)
-                launch(d, "hub_apply_kernel", hub_apply_kernel<W, C>, static_cast<int>(hubs.chunks), kThreads, 0,
-                       hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
+                launch(d, "hub_apply_kernel", hub_apply_kernel<W, C>,
+                       static_cast<int>(std::min<i64>(hubs.chunks, static_cast<i64>(d.sms) * 8)), kThreads, 0,
+                       hubs.chunks, hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
         }
-        launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, c0.movers), kThreads, 0, w.movers.get(), ctr, labels,
+        launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, bound), kThreads, 0, w.movers.get(), ctr, labels,
                w.targets.get(), vw, pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
         if (rebuild) build_cache();
         trace().mark(d, rebuild ? "refine.rebuild" : "refine.apply", c0.movers, c0.mover_degree);
@@ -1067,6 +1075,16 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         GP_CUDA(cudaMemcpyAsync(stats_dev.get()->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
         Stats h;
         fetch(d, &h, stats_dev.get(), 1);
+        if (d.prof && !rebuild) {
+            // per mover: offsets, label and target; per mover edge: neighbour,
+            // weight, the neighbour's label and two read-modify-writes of the cache
+            const double per_mover = 2 * sizeof(O) + 4 + 4 + 4;
+            const double per_edge = 4 + 4 + (ew ? sizeof(W) : 0) + 4 * sizeof(C);
+            d.prof_bytes("apply_cache_cut_kernel", static_cast<double>(h.c.movers - h.c.big) * per_mover +
+                                                       static_cast<double>(h.c.walked_degree) * per_edge);
+            d.prof_bytes("apply_big_rows_kernel",
+                         static_cast<double>(h.c.big) * per_mover + static_cast<double>(h.c.big_degree) * per_edge);
+        }
         if (rebuild) {
             current_cut = undirected_cut(d, g, labels, w.scratch.get());
         } else {
@@ -1086,7 +1104,6 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         }
         return h.c.movers;
     };
-    i64 ncand = 0;   // rebalance candidates in w.cand (vertices of overloaded parts, ascending)
     auto deterministic_ranks = [&]() {
         // candidates in ascending vertex order, sorted by (bucket, gpw desc)
         exclusive_scan<i64>(d, HasBucket{w.bucket.get(), w.cand.get()}, w.pos.get(), ncand,
@@ -1765,6 +1782,7 @@ void gp_ctx_destroy(gp_ctx* ctx) {
     for (auto& kv : d.live) cudaFree(kv.first);
     d.live.clear();
     for (auto e : d.event_pool) cudaEventDestroy(e);
+    if (d.sync_event) cudaEventDestroy(d.sync_event);
     if (d.err) cudaFree(d.err);
     if (d.pinned) cudaFreeHost(d.pinned);
     if (d.stream) cudaStreamDestroy(d.stream);
@@ -1772,6 +1790,17 @@ void gp_ctx_destroy(gp_ctx* ctx) {
 }
 
 const char* gp_ctx_error(const gp_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+gp_status gp_ctx_set_sync_mode(gp_ctx* ctx, int blocking) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        auto& d = ctx->dev;
+        GP_CUDA(cudaSetDevice(d.device));
+        if (blocking && !d.sync_event)
+            GP_CUDA(cudaEventCreateWithFlags(&d.sync_event, cudaEventBlockingSync | cudaEventDisableTiming));
+        d.blocking_sync = blocking != 0;
+    });
+}
 
 gp_status gp_partition_capacity(uint64_t total, int parts, double ratio, uint64_t* out) {
     return guarded(nullptr, [&] { *out = gp::partition_capacity(total, parts, ratio); });
@@ -2172,6 +2201,7 @@ gp_status gp_refine(gp_ctx* ctx, const gp_graph* graph, int32_t* labels, int par
 }
 
 uint64_t gp_launch_count(const gp_ctx* ctx) { return ctx ? ctx->dev.launches : 0; }
+uint64_t gp_sync_count(const gp_ctx* ctx) { return ctx ? ctx->dev.syncs : 0; }
 
 gp_status gp_initial_partition_static(const gp_graph* graph, int parts, double ratio, uint32_t seed, int32_t* labels,
                                       void* stream, char* message, uint64_t message_capacity) {

@@ -27,7 +27,9 @@ struct RefineCounters {
     long long delta;      // cut decrease of the last apply
     u64 directed_cut;
     i64 mover_degree;     // sum of the movers' degrees
-    u64 pad[3];
+    i64 big;              // movers of degree > kSplitDegree handed to apply_big_rows_kernel
+    i64 big_degree;       // their degree sum
+    i64 walked_degree;    // edges apply_cache_cut_kernel walked itself
 };
 
 // Per-vertex proposal record written by the LP pass: the priority filter
@@ -246,15 +248,42 @@ __global__ void __launch_bounds__(kThreads) priority_filter_kernel(
     }
 }
 
-// incremental_update_cache_and_cut (src/refine_incremental.cuh:69-95)
+// incremental_update_cache_and_cut (src/refine_incremental.cuh:69-95).  One
+// edge of mover v (label s, target t): the neighbour's cache row loses w at s
+// and gains it at t; the cut change is counted once per undirected edge (the
+// neighbour is not a mover, or has the larger id).
+template <typename W, typename C>
+__device__ __forceinline__ long long apply_edge(i32 v, i32 s, i32 t, i64 e, const i32* __restrict__ nbr,
+                                                const W* __restrict__ ew, const i32* __restrict__ labels,
+                                                const i32* __restrict__ targets,
+                                                const unsigned char* __restrict__ flags, int k, C* cache) {
+    const i32 u = nbr[e];
+    if (u == v) return 0;
+    const u64 w = static_cast<u64>(weight_at(ew, e));
+    const bool fu = flags[u] != 0;
+    const i32 lu = labels[u];
+    cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
+    cache_add(&cache[static_cast<i64>(u) * k + t], w);
+    if (fu && u < v) return 0;
+    const i32 nn = fu ? targets[u] : lu;
+    return static_cast<long long>(w) * ((s != lu) - (t != nn));
+}
+
+// Movers of degree above this are walked by a whole block
+// (apply_big_rows_kernel): one warp would take deg/32 dependent steps, and the
+// launch would wait for that one warp.
+constexpr i64 kSplitDegree = 256;
+
 template <typename O, typename W, typename C>
 __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
     const i32* __restrict__ movers, const RefineCounters* ctr_in, const O* __restrict__ off,
     const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
-    const i32* __restrict__ targets, const unsigned char* __restrict__ flags, int k, C* cache, RefineCounters* ctr) {
-    // A warp takes up to 32 movers and walks their edges together (hub rows:
-    // chunked kernel).  The cut delta is summed per warp and added with one
-    // atomic per warp, so warps never wait for each other.
+    const i32* __restrict__ targets, const unsigned char* __restrict__ flags, int k, C* cache, RefineCounters* ctr,
+    i32* __restrict__ big) {
+    // A warp takes up to 32 movers and walks their edges together (rows above
+    // kSplitDegree: block kernel; hub rows: chunked kernel).  The cut delta is
+    // summed per warp and added with one atomic per warp, so warps never wait
+    // for each other.
     const int lane = threadIdx.x & 31;
     const i64 count = ctr_in->movers;
     const i64 warps = static_cast<i64>(gridDim.x) * kWarps;
@@ -266,28 +295,48 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
         const i32 v = has ? movers[i] : 0;
         const i64 b = has ? static_cast<i64>(off[v]) : 0;
         i64 deg = has ? static_cast<i64>(off[v + 1]) - b : 0;
-        if (deg > kHubDegree) deg = 0;
+        const bool split = deg > kSplitDegree && deg <= kHubDegree;
+        const u64 slot = warp_append(split, reinterpret_cast<u64*>(&ctr->big));
+        if (split) big[slot] = v;
+        const i64 big_degree = warp_sum(split ? deg : i64{0});
+        if (lane == 0 && big_degree)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->big_degree), static_cast<unsigned long long>(big_degree));
+        if (deg > kSplitDegree) deg = 0;
+        const i64 walked = warp_sum(deg);
+        if (lane == 0 && walked)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->walked_degree), static_cast<unsigned long long>(walked));
         const i32 s = has ? labels[v] : 0, t = has ? targets[v] : 0;
         warp_edge_walk(b, deg, [&](bool valid, int owner, i64 e) {
             const i32 ov = __shfl_sync(0xffffffffu, v, owner);
             const i32 os = __shfl_sync(0xffffffffu, s, owner);
             const i32 ot = __shfl_sync(0xffffffffu, t, owner);
-            if (!valid) return;
-            const i32 u = nbr[e];
-            if (u == ov) return;
-            const u64 w = static_cast<u64>(weight_at(ew, e));
-            const bool fu = flags[u] != 0;
-            const i32 lu = labels[u];
-            cache_add(&cache[static_cast<i64>(u) * k + os], 0ULL - w);
-            cache_add(&cache[static_cast<i64>(u) * k + ot], w);
-            if (!fu || u > ov) {
-                const i32 nn = fu ? targets[u] : lu;
-                gain += static_cast<long long>(w) * ((os != lu) - (ot != nn));
-            }
+            if (valid) gain += apply_edge(ov, os, ot, e, nbr, ew, labels, targets, flags, k, cache);
         });
     }
     gain = warp_sum(gain);
     if (lane == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));
+}
+
+// The movers set aside by apply_cache_cut_kernel (kSplitDegree < degree <=
+// kHubDegree), one block per row over a grid-stride loop.
+template <typename O, typename W, typename C>
+__global__ void __launch_bounds__(kThreads) apply_big_rows_kernel(
+    const i32* __restrict__ big, const RefineCounters* ctr_in, const O* __restrict__ off,
+    const i32* __restrict__ nbr, const W* __restrict__ ew, const i32* __restrict__ labels,
+    const i32* __restrict__ targets, const unsigned char* __restrict__ flags, int k, C* cache, RefineCounters* ctr) {
+    __shared__ long long sh[kWarps + 1];
+    const i64 count = ctr_in->big;
+    long long gain = 0;
+    for (i64 r = blockIdx.x; r < count; r += gridDim.x) {
+        const i32 v = big[r];
+        const i32 s = labels[v], t = targets[v];
+        const i64 e1 = static_cast<i64>(off[v + 1]);
+        for (i64 e = static_cast<i64>(off[v]) + threadIdx.x; e < e1; e += kThreads)
+            gain += apply_edge(v, s, t, e, nbr, ew, labels, targets, flags, k, cache);
+    }
+    gain = block_sum(gain, sh);
+    if (threadIdx.x == 0 && gain)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));
 }
 
 // incremental_commit (src/refine_incremental.cuh:97-109); also clears the

@@ -198,6 +198,13 @@ gp_status gp_cut(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int 
 /* Kernel launches issued by this context so far (all of them are the
  * library's own sm_100a kernels). */
 uint64_t gp_launch_count(const gp_ctx* ctx);
+/* Host waits on the context's stream so far (device-to-host round trips). */
+uint64_t gp_sync_count(const gp_ctx* ctx);
+/* How the host thread waits for the context's stream: 0 (default) polls,
+ * which gives the lowest latency per round trip; 1 sleeps until the work is
+ * done, which frees the core for other host threads when many contexts run
+ * at once (the server's slots). */
+gp_status gp_ctx_set_sync_mode(gp_ctx* ctx, int blocking);
 
 /* Spectral initial partition that allocates no device memory.
  *
