@@ -352,6 +352,10 @@ class Context:
     def syncs(self) -> int:
         return int(lib().gp_sync_count(self._h))
 
+    def set_sync_mode(self, blocking: bool):
+        """Host waits sleep (True) or poll (False, the default)."""
+        self._check(lib().gp_ctx_set_sync_mode(self._h, int(blocking)))
+
     @property
     def stream(self) -> int:
         return int(lib().gp_ctx_stream(self._h) or 0)

@@ -88,10 +88,17 @@ struct DGraph {
     mutable int unique_rows = -1;
 };
 
+// known_count: the number of hub vertices when the caller already has it
+// (the degree classes of an aggregation); 0 skips the scans.
 template <typename T>
-const typename DGraph<T>::Hubs& hub_index(Device& d, const DGraph<T>& g) {
+const typename DGraph<T>::Hubs& hub_index(Device& d, const DGraph<T>& g, i64 known_count = -1) {
     auto& h = g.hubs;
     if (h.built) return h;
+    if (known_count == 0) {
+        h.count = h.chunks = 0;
+        h.built = true;
+        return h;
+    }
     using O = typename T::O;
     const i64 n = g.n;
     Buf<i64> hpos(d, static_cast<size_t>(n) + 1), cpos(d, static_cast<size_t>(n) + 1), tot(d, 2);
@@ -311,11 +318,10 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         w.edge_total_known = true;
     }
     const int sum32 = w.edge_total <= 0xffffffffULL ? 1 : 0;
+    const auto& hubs = hub_index(d, g, static_cast<i64>(cnt[5]));
     // hash-free affinity on identity rounds (rows without duplicates)
     const bool direct_ok = unique_rows(d, g);
     // global hash tables for hubs
-
-    const auto& hubs = hub_index(d, g);
     if (hubs.count != static_cast<i64>(cnt[5])) fail(GP_ERUNTIME, "hub index disagrees with degree classes");
     i64 table_total = 0;
     if (hubs.count > 0) {
@@ -968,9 +974,14 @@ struct RefineWork {
     }
 };
 
+// known_cut: the cut of `labels` when the caller has it (a projection keeps
+// the cut of the coarser level's result), else kUnknownCut.
+constexpr u64 kUnknownCut = ~0ULL;
+
 template <typename T, typename C>
 gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* labels, u64* pw,
-                             std::vector<u64>& host_pw, int k, u64 cap, int rounds, bool deterministic, bool verify) {
+                             std::vector<u64>& host_pw, int k, u64 cap, int rounds, bool deterministic, bool verify,
+                             u64 known_cut) {
     using O = typename T::O;
     using W = typename T::W;
     const i64 n = g.n;
@@ -1001,7 +1012,7 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         hub_corr.zero(d);
     }
     GP_LAUNCH();
-    u64 current_cut = undirected_cut(d, g, labels, w.scratch.get());
+    u64 current_cut = known_cut != kUnknownCut ? known_cut : undirected_cut(d, g, labels, w.scratch.get());
     st.initial_cut = current_cut;
     u64 best_cut = current_cut;
     auto checkpoint = [&]() {
@@ -1010,17 +1021,18 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     };
     checkpoint();
     auto maximum = [&]() { return *std::max_element(host_pw.begin(), host_pw.end()); };
-    // maximum edge weight decides the LP filter (refine_incremental.cuh:332-333)
-    u64 maxe = 1;
+    // maximum edge weight decides the LP filter (refine_incremental.cuh:332-333);
+    // for weighted levels it stays on the device (w.scratch[7]) and the LP
+    // kernel derives the filter from it
+    const double filter = 0.25;
+    const u64* max_edge_weight = nullptr;
     if (ew) {
-        GP_CUDA(cudaMemsetAsync(w.scratch.get(), 0, sizeof(u64), d.stream));
-        launch(d, "max_weight_kernel", max_weight_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, ew, w.scratch.get());
+        GP_CUDA(cudaMemsetAsync(w.scratch.get() + 7, 0, sizeof(u64), d.stream));
+        launch(d, "max_weight_kernel", max_weight_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, ew,
+               w.scratch.get() + 7);
         GP_LAUNCH();
-        fetch(d, &maxe, w.scratch.get(), 1);
-    } else if (g.m == 0) {
-        maxe = 0;
+        max_edge_weight = w.scratch.get() + 7;
     }
-    const double filter = maxe <= 1 ? 0.25 : 0.75;
     struct Stats { RefineCounters c; u64 pw[32]; };
     Buf<Stats> stats_dev(d, 1);
     auto build_cache = [&]() {
@@ -1041,7 +1053,7 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     // stay edge by edge: measured, the rebuild plus recount does not pay
     // there.)  The kernels read the mover count from the device, so a
     // rebalance apply needs no round trip before its launch: its grids are
-    // sized for the candidate count, an upper bound of its movers.
+    // sized for an upper bound of its movers.
     i64 ncand = 0;   // rebalance candidates in w.cand (vertices of overloaded parts, ascending)
     auto finish_apply = [&](bool lp) -> i64 {
         RefineCounters c0{};
@@ -1133,31 +1145,38 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     };
     auto rebalance = [&]() -> bool {
         if (maximum() <= cap) return true;
-        exclusive_scan<i64>(d, InOverloaded{labels, pw, cap}, w.pos.get(), n,
-                            reinterpret_cast<i64*>(w.scratch.get() + 1));
+        i64* cand_count = reinterpret_cast<i64*>(w.scratch.get() + 6);
+        exclusive_scan<i64>(d, InOverloaded{labels, pw, cap}, w.pos.get(), n, cand_count);
         launch(d, "compact_overloaded_kernel", compact_overloaded_kernel, blocks_for(n, kThreads), kThreads, 0, n,
                labels, pw, cap, w.pos.get(), w.cand.get());
-        fetch(d, &ncand, reinterpret_cast<i64*>(w.scratch.get() + 1), 1);
-        const int cgrid = blocks_for(std::max<i64>(ncand, 1), kThreads);
+        // The candidate count stays on the device unless the host needs it
+        // (the deterministic ranks size their sorts by it): the kernels read
+        // it, and the grids are sized for the level's n.
+        const bool host_count = deterministic || d.prof || trace().on;
+        if (host_count) fetch(d, &ncand, cand_count, 1);
+        else ncand = n;
+        const i64* dev_count = host_count ? nullptr : cand_count;
+        const int cgrid = host_count ? blocks_for(std::max<i64>(ncand, 1), kThreads) : stride_grid(d, n);
         for (int it = 0; it < 2 * k + 4 && maximum() > cap; ++it) {
             ++st.admission_iterations;
             GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
             w.counts.zero(d);
             launch(d, "rebalance_proposals_kernel", rebalance_proposals_kernel<C, W>, cgrid, kThreads, 0, ncand,
-                   w.cand.get(), cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(),
+                   dev_count, w.cand.get(), cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(),
                    w.gpw.get(), w.bucket.get(), w.rank.get(), w.counts.get());
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
             w.counts.zero(d);
-            launch(d, "select_sources_kernel", select_sources_kernel<W>, cgrid, kThreads, 0, ncand, w.cand.get(),
+            launch(d, "select_sources_kernel", select_sources_kernel<W>, cgrid, kThreads, 0, ncand, dev_count,
+                   w.cand.get(),
                    w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, w.targets.get(), vw, deterministic ? 1 : 0,
                    w.counts.get());
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
             launch(d, "select_destinations_kernel", select_destinations_kernel<W>, cgrid, kThreads, 0, ncand,
-                   w.cand.get(), w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(),
+                   dev_count, w.cand.get(), w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(),
                    w.movers.get(), ctr);
             GP_LAUNCH();
             const i64 moved = finish_apply(false);
@@ -1171,7 +1190,7 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
         d.prof_bytes("lp_proposals_kernel", static_cast<double>(n) * (k * sizeof(C) + 4 + 1 + 4 + 8));
         launch(d, "lp_proposals_kernel", lp_proposals_kernel<C>, blocks_for(n, kThreads), kThreads, 0, n, cache, labels, k,
-               filter, w.locks.get(), w.targets.get(), w.gains.get(), w.props.get(), w.list.get(), ctr);
+               filter, max_edge_weight, w.locks.get(), w.targets.get(), w.gains.get(), w.props.get(), w.list.get(), ctr);
         launch(d, "priority_filter_kernel", priority_filter_kernel<O, W>, stride_grid(d, n * 32), kThreads, 0,
                w.list.get(), ctr, off, nbr, ew, w.props.get(), w.flags.get(), w.movers.get(), ctr);
         if (hubs.count) {
@@ -1208,36 +1227,43 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     return st;
 }
 
-// The affinity cache can hold 32-bit sums when the level's total directed
-// edge weight fits in 32 bits (whatever the graph width): no row sum can
-// exceed it.
+// Total directed edge weight of a level, saturated at 2^64 - 1 (m for unit
+// weights, without a pass over the edges).
 template <typename T>
-bool narrow_cache(const DGraph<T>& g, Device& d) {
+u64 directed_total(Device& d, const DGraph<T>& g) {
+    if (!g.ewp()) return static_cast<u64>(g.m);
     Buf<u64> s(d, 1);
     s.zero(d);
     launch(d, "sat_sum_kernel", sat_sum_kernel<typename T::W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), s.get());
     GP_LAUNCH();
     u64 total = 0;
     fetch(d, &total, s.get(), 1);
-    return total <= 0xffffffffULL;
+    return total;
 }
 
+// The affinity cache can hold 32-bit sums when the level's total directed
+// edge weight fits in 32 bits (whatever the graph width): no row sum can
+// exceed it.
+template <typename T>
+bool narrow_cache(const DGraph<T>& g, Device& d) { return directed_total(d, g) <= 0xffffffffULL; }
+
+// validate_refinement_gain_range (src/refine.cu:346-383): only the big width
+// can exceed INT64_MAX/2 in total directed weight.
+template <typename T>
+void check_gain_range(u64 directed_total) {
+    if (sizeof(typename T::W) == 8 && directed_total > static_cast<u64>(INT64_MAX) / 2)
+        fail(GP_EOVERFLOW, "refinement signed gain range exceeded");
+}
+
+// range_checked: the caller ran check_gain_range on a level at least as heavy
+// (a contraction only drops internal edges, so coarser levels weigh less).
 template <typename T>
 gp_refine_stats refine_dispatch(Device& d, const DGraph<T>& g, RefineWork& w, i32* labels, u64* pw,
-                                std::vector<u64>& host_pw, int k, u64 cap, int rounds, bool det, bool verify, bool narrow) {
-    // validate_refinement_gain_range (src/refine.cu:346-383): only the big
-    // width can exceed INT64_MAX/2 in total directed weight.
-    if constexpr (sizeof(typename T::W) == 8) {
-        Buf<u64> s(d, 1);
-        s.zero(d);
-        launch(d, "sat_sum_kernel", sat_sum_kernel<typename T::W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), s.get());
-        GP_LAUNCH();
-        u64 total = 0;
-        fetch(d, &total, s.get(), 1);
-        if (total > static_cast<u64>(INT64_MAX) / 2) fail(GP_EOVERFLOW, "refinement signed gain range exceeded");
-    }
-    if (narrow) return refine_level<T, u32>(d, g, w, labels, pw, host_pw, k, cap, rounds, det, verify);
-    return refine_level<T, u64>(d, g, w, labels, pw, host_pw, k, cap, rounds, det, verify);
+                                std::vector<u64>& host_pw, int k, u64 cap, int rounds, bool det, bool verify, bool narrow,
+                                bool range_checked = false, u64 known_cut = kUnknownCut) {
+    if (!range_checked && sizeof(typename T::W) == 8) check_gain_range<T>(directed_total(d, g));
+    if (narrow) return refine_level<T, u32>(d, g, w, labels, pw, host_pw, k, cap, rounds, det, verify, known_cut);
+    return refine_level<T, u64>(d, g, w, labels, pw, host_pw, k, cap, rounds, det, verify, known_cut);
 }
 
 template <typename T>
@@ -1264,12 +1290,17 @@ void uncoarsen(Device& d, Hierarchy<T>& h, Buf<i32>& labels, const Opts& o, u64 
     Buf<u64> pw(d, 32);
     std::vector<u64> host_pw;
     auto& coarsest = h.levels.back();
-    const bool narrow = narrow_cache(coarsest, d) && narrow_cache(h.levels.front(), d);
+    // The finest level is the heaviest (a contraction only drops internal
+    // edges), so its total decides the cache width and the gain range of
+    // every level, and it is the reported total edge weight.
+    const u64 directed = directed_total(d, h.levels.front());
+    const bool narrow = directed <= 0xffffffffULL;
     part_weights(d, coarsest, labels.get(), k, pw.get(), host_pw);
     if (*std::max_element(host_pw.begin(), host_pw.end()) > cap)
         fail(GP_EINVAL, "initial refinement partition is imbalanced");
+    check_gain_range<T>(directed);
     auto st = refine_dispatch(d, coarsest, work, labels.get(), pw.get(), host_pw, k, cap, o.max_rounds,
-                              o.deterministic, o.verify, narrow);
+                              o.deterministic, o.verify, narrow, true);
     u64 last_cut = st.final_cut;
     i64 last_refined = coarsest.n;
     if (log.on)
@@ -1297,7 +1328,7 @@ void uncoarsen(Device& d, Hierarchy<T>& h, Buf<i32>& labels, const Opts& o, u64 
         gp_refine_stats ls{};
         if (refine_this) {
             ls = refine_dispatch(d, fine, work, labels.get(), pw.get(), host_pw, k, cap, o.max_rounds,
-                                 o.deterministic, o.verify, narrow);
+                                 o.deterministic, o.verify, narrow, true, last_cut);
             last_refined = fine.n;
         } else {
             ls.initial_cut = ls.final_cut = last_cut;
@@ -1311,17 +1342,6 @@ void uncoarsen(Device& d, Hierarchy<T>& h, Buf<i32>& labels, const Opts& o, u64 
                     << " admission_iterations=" << ls.admission_iterations
                     << " admission_fallbacks=" << ls.admission_fallbacks << " refined_cut=" << ls.final_cut
                     << " refined_max_part_weight=" << ls.final_max_part_weight << '\n';
-    }
-    auto& finest = h.levels.front();
-    u64 directed = 0;
-    if (finest.ewp()) {
-        Buf<u64> s(d, 1);
-        s.zero(d);
-        launch(d, "sum_weight_kernel", sum_weight_kernel<typename T::W>, stride_grid(d, finest.m), kThreads, 0, finest.m, finest.ewp(), s.get());
-        GP_LAUNCH();
-        fetch(d, &directed, s.get(), 1);
-    } else {
-        directed = static_cast<u64>(finest.m);
     }
     if (directed & 1ULL) fail(GP_ERUNTIME, "symmetric graph has odd directed edge weight");
     r.cut = last_cut;

@@ -152,9 +152,12 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
 // are appended to `list`.
 template <typename C>
 __global__ void lp_proposals_kernel(i64 n, const C* __restrict__ cache, const i32* __restrict__ labels, int k,
-                                    double filter, unsigned char* locks, i32* targets, i64* gains, PropRec* props,
-                                    i32* list, RefineCounters* ctr) {
+                                    double filter, const u64* __restrict__ max_edge_weight, unsigned char* locks,
+                                    i32* targets, i64* gains, PropRec* props, i32* list, RefineCounters* ctr) {
     const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    // the filter of refine_incremental.cuh:332-333, from the level's maximum
+    // edge weight when it was computed on the device
+    if (max_edge_weight) filter = *max_edge_weight <= 1 ? 0.25 : 0.75;
     bool propose = false;
     if (v < n) {
         i32 target = -1;
@@ -476,24 +479,32 @@ __device__ __forceinline__ int rebalance_choice(i64 v, const C* __restrict__ cac
     return b;
 }
 
+// The rebalance kernels run over list[0, n), or over list[0, *count) when
+// `count` is given (the candidate count left on the device, no round trip);
+// their grid-stride loops keep whole warps together for the warp ranks.
+__device__ __forceinline__ i64 list_length(i64 n, const i64* count) { return count ? *count : n; }
+
 // Over the candidate list (vertices of overloaded parts); part weights are
 // staged in shared memory.
 template <typename C, typename W>
-__global__ void rebalance_proposals_kernel(i64 n, const i32* __restrict__ list, const C* __restrict__ cache,
-                                           const i32* __restrict__ labels, const W* __restrict__ vw, int k,
-                                           const u64* __restrict__ pw, u64 cap, BucketThresholds th,
-                                           int deterministic, i32* targets, double* gpw, i32* bucket, u64* rank,
-                                           u64* counts) {
+__global__ void rebalance_proposals_kernel(i64 n, const i64* count, const i32* __restrict__ list,
+                                           const C* __restrict__ cache, const i32* __restrict__ labels,
+                                           const W* __restrict__ vw, int k, const u64* __restrict__ pw, u64 cap,
+                                           BucketThresholds th, int deterministic, i32* targets, double* gpw,
+                                           i32* bucket, u64* rank, u64* counts) {
     __shared__ u64 spw[32];
     if (threadIdx.x < 32) spw[threadIdx.x] = static_cast<int>(threadIdx.x) < k ? pw[threadIdx.x] : ~0ULL;
     __syncthreads();
-    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const i64 v = i < n ? (list ? list[i] : i) : 0;
-    u64 w = 0;
-    const int b = i < n ? rebalance_choice(v, cache, labels, vw, k, spw, cap, th, targets, gpw, bucket, w) : -1;
-    if (!deterministic) {
-        const u64 r = warp_rank_add(b, w, vw == nullptr, counts);
-        if (b >= 0) rank[v] = r;
+    n = list_length(n, count);
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < n; base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 i = base + threadIdx.x;
+        const i64 v = i < n ? (list ? list[i] : i) : 0;
+        u64 w = 0;
+        const int b = i < n ? rebalance_choice(v, cache, labels, vw, k, spw, cap, th, targets, gpw, bucket, w) : -1;
+        if (!deterministic) {
+            const u64 r = warp_rank_add(b, w, vw == nullptr, counts);
+            if (b >= 0) rank[v] = r;
+        }
     }
 }
 
@@ -521,48 +532,54 @@ __global__ void __launch_bounds__(kThreads) bucket_scan_kernel(const u64* counts
 
 // balance_select_sources (src/refine_incremental.cuh:204-217)
 template <typename W>
-__global__ void select_sources_kernel(i64 n, const i32* __restrict__ list, i32* bucket, u64* rank, const u64* offsets,
-                                      const u64* pw, u64 cap, const i32* targets, const W* vw, int deterministic,
-                                      u64* counts) {
-    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const i64 v = i < n ? (list ? list[i] : i) : 0;
-    int d = -1;
-    if (i < n && bucket[v] >= 0) {
-        const int b = bucket[v], s = b / kBalWidth;
-        if (offsets[b] + rank[v] >= pw[s] - cap) {
-            bucket[v] = -1;
-        } else {
-            d = targets[v] * kBalWidth + b % kBalWidth;
-            bucket[v] = d;
+__global__ void select_sources_kernel(i64 n, const i64* count, const i32* __restrict__ list, i32* bucket, u64* rank,
+                                      const u64* offsets, const u64* pw, u64 cap, const i32* targets, const W* vw,
+                                      int deterministic, u64* counts) {
+    n = list_length(n, count);
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < n; base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 i = base + threadIdx.x;
+        const i64 v = i < n ? (list ? list[i] : i) : 0;
+        int d = -1;
+        if (i < n && bucket[v] >= 0) {
+            const int b = bucket[v], s = b / kBalWidth;
+            if (offsets[b] + rank[v] >= pw[s] - cap) {
+                bucket[v] = -1;
+            } else {
+                d = targets[v] * kBalWidth + b % kBalWidth;
+                bucket[v] = d;
+            }
         }
-    }
-    if (!deterministic) {
-        const u64 r = warp_rank_add(d, i < n ? static_cast<u64>(weight_at(vw, v)) : 0, vw == nullptr, counts);
-        if (d >= 0) rank[v] = r;
+        if (!deterministic) {
+            const u64 r = warp_rank_add(d, i < n ? static_cast<u64>(weight_at(vw, v)) : 0, vw == nullptr, counts);
+            if (d >= 0) rank[v] = r;
+        }
     }
 }
 
 // balance_select_destinations (src/refine_incremental.cuh:219-232).
 template <typename W>
-__global__ void select_destinations_kernel(i64 n, const i32* __restrict__ list, const i32* bucket, const u64* rank,
-                                           const u64* offsets, const u64* pw, u64 cap, const W* vw,
+__global__ void select_destinations_kernel(i64 n, const i64* count, const i32* __restrict__ list, const i32* bucket,
+                                           const u64* rank, const u64* offsets, const u64* pw, u64 cap, const W* vw,
                                            unsigned char* flags, i32* movers, RefineCounters* ctr) {
-    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool move = false;
-    i64 v = 0;
-    if (i < n) {
-        v = list ? list[i] : i;
-        const int b = bucket[v];
-        if (b >= 0) {
-            const u64 before = offsets[b] + rank[v];
-            const u64 slack = cap - pw[b / kBalWidth];
-            move = before <= slack && static_cast<u64>(weight_at(vw, v)) <= slack - before;
+    n = list_length(n, count);
+    for (i64 base = static_cast<i64>(blockIdx.x) * blockDim.x; base < n; base += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i64 i = base + threadIdx.x;
+        bool move = false;
+        i64 v = 0;
+        if (i < n) {
+            v = list ? list[i] : i;
+            const int b = bucket[v];
+            if (b >= 0) {
+                const u64 before = offsets[b] + rank[v];
+                const u64 slack = cap - pw[b / kBalWidth];
+                move = before <= slack && static_cast<u64>(weight_at(vw, v)) <= slack - before;
+            }
         }
-    }
-    const u64 slot = warp_append(move, reinterpret_cast<u64*>(&ctr->movers));
-    if (move) {
-        flags[v] = 1;
-        movers[slot] = static_cast<i32>(v);
+        const u64 slot = warp_append(move, reinterpret_cast<u64*>(&ctr->movers));
+        if (move) {
+            flags[v] = 1;
+            movers[slot] = static_cast<i32>(v);
+        }
     }
 }
 

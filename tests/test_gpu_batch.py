@@ -110,6 +110,17 @@ def test_server_admission_budget():
         assert s1 >= e0 - 1e-3
 
 
+def test_blocking_sync_mode_same_labels(ctx):
+    off, nbr = graphs.rmat_csr(13, 16, 5)
+    la, ra = alone(ctx, off, nbr, 8)
+    with hb.Context(0) as c:
+        c.set_sync_mode(True)
+        s0 = c.syncs
+        lb, rb = alone(c, off, nbr, 8)
+        assert c.syncs > s0
+    assert np.array_equal(la, lb) and ra.cut == rb.cut
+
+
 @pytest.mark.parametrize("make,k", [(lambda: graphs.rmat_csr(16, 16, 1), 32), (lambda: graphs.grid2d_csr(300, 300), 4),
                                     (lambda: graphs.rgg_csr(100000, 10.0, 3), 16)])
 def test_footprint_bounds_measured_peak(make, k):
