@@ -123,6 +123,26 @@ __device__ __forceinline__ void slot_insert(S* table, u32 size, i32 c, u64 w, u3
     set_error(err, kErrTableFull);
 }
 
+// 8-byte slots: key and value are claimed together by one 64-bit CAS (an
+// empty slot is the all-zero word), so a first insert is a single atomic; a
+// slot that already holds the key takes a 32-bit add.
+__device__ __forceinline__ void slot_insert(HubSlot32* table, u32 size, i32 c, u64 w, u32* err) {
+    const u32 key = static_cast<u32>(c) + 1;
+    const unsigned long long fresh = (static_cast<unsigned long long>(static_cast<u32>(w)) << 32) | key;
+    u32 slot = slot_of(c, size);
+    for (u32 probe = 0; probe < size; ++probe) {
+        const unsigned long long found =
+            atomicCAS(reinterpret_cast<unsigned long long*>(&table[slot]), 0ULL, fresh);
+        if (found == 0ULL) return;
+        if (static_cast<u32>(found) == key) {
+            table[slot].add(w);
+            return;
+        }
+        if (++slot == size) slot = 0;
+    }
+    set_error(err, kErrTableFull);
+}
+
 template <typename O, typename W, typename S>
 __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
     const Chunk* __restrict__ chunks, const i32* __restrict__ nbr, const W* __restrict__ ew,
