@@ -163,6 +163,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes per algorithmic byte, measured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum over every launch of the kernel in one timed
+# partition of RMAT-20 ef16, k=32, against the library's algorithmic bytes for
+# the same launches).  The traffic of a launch here is that ratio times its
+# algorithmic bytes.
+DRAM_PER_ALGORITHMIC_BYTE = {"hub_insert_kernel": 1.745, "segment_smem_kernel": 0.555}
+
+
 # Algorithmic bytes per launch of the dominant kernels are recorded by the
 # library itself (gp_profile_dump); this picks the kernel with the largest
 # total time that has a traffic model.
@@ -172,10 +180,15 @@ def roofline(profile: dict, hbm_gbs: float, src: str):
     for name, v in ranked:
         if v["bytes"] > 0 and v["ms"] > 0:
             achieved = v["bytes"] / (v["ms"] * 1e-3) / 1e9
+            per_launch = v["bytes"] / max(1, v["launches"])
+            ratio = DRAM_PER_ALGORITHMIC_BYTE.get(name)
             return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_gbs,
-                    "peak_source": src, "unit": "GB/s", "frac": round(achieved / hbm_gbs, 4), "traffic": None,
+                    "peak_source": src, "unit": "GB/s", "frac": round(achieved / hbm_gbs, 4),
+                    "traffic": round(ratio * per_launch) if ratio else None,
+                    "traffic_source": ("ncu DRAM bytes per algorithmic byte of this kernel on RMAT-20 "
+                                       f"({ratio}) x the algorithmic bytes per launch here") if ratio else None,
                     "share_of_gpu_time": round(v["ms"] / total_ms, 4), "launches": v["launches"],
-                    "algorithmic_bytes_per_launch": v["bytes"] / max(1, v["launches"])}
+                    "algorithmic_bytes_per_launch": per_launch}
     return None
 
 

@@ -181,6 +181,32 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
 
 struct HubPartial { u64 current, best, tie; };
 
+// Profiling only: the work an affinity pass over `list` really does, since
+// vertices (and hubs) whose own cluster is not a mover are skipped.  out[0]
+// counts the processed vertices, out[1] their edges, out[2] the slots of
+// their hub tables (HubTableSize).
+template <typename O>
+__global__ void role_work_kernel(i64 count, const i32* __restrict__ list, const O* __restrict__ off,
+                                 const i32* __restrict__ clusters, RoundParams p, u64* out) {
+    u64 v_n = 0, e_n = 0, s_n = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i32 v = list[i];
+        if (role_blocked(p.identity ? v : clusters[v], p)) continue;
+        const i64 d = static_cast<i64>(off[v + 1]) - off[v];
+        const i64 want = d + (d * 3 + 9) / 10;
+        ++v_n;
+        e_n += static_cast<u64>(d);
+        s_n += static_cast<u64>((want + kSlotTile - 1) / kSlotTile * kSlotTile);
+    }
+    v_n = warp_sum(v_n); e_n = warp_sum(e_n); s_n = warp_sum(s_n);
+    if ((threadIdx.x & 31) == 0 && v_n) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(out), static_cast<unsigned long long>(v_n));
+        atomicAdd(reinterpret_cast<unsigned long long*>(out + 1), static_cast<unsigned long long>(e_n));
+        atomicAdd(reinterpret_cast<unsigned long long*>(out + 2), static_cast<unsigned long long>(s_n));
+    }
+}
+
 template <typename W, typename S>
 __global__ void __launch_bounds__(kThreads) hub_candidates_kernel(
     i64 hubs, const i32* __restrict__ hub_list, const i64* __restrict__ table_off, S* table,

@@ -296,7 +296,6 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     u32 cnt[kClasses];
     to_host(d, stats, sc, 16);
     fetch(d, cnt, w.ccount.get(), kClasses);
-    const u64* class_edges = stats + 8;
     const u64 total = stats[0], maxw = stats[1];
     const u64 denom = static_cast<u64>(beta) * static_cast<u64>(parts);
     const u64 cap = std::max(maxw, total / denom + (total % denom != 0 ? 1 : 0));
@@ -345,19 +344,32 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     GP_LAUNCH();
     SclpOut so{w.target.get(), w.gain.get(), w.tie.get(), w.demand.get()};
 
-    // Algorithmic bytes of one affinity+decode pass over class c: offsets,
-    // list, neighbours, edge weights, cluster gathers (none at round 0),
-    // cluster[v]/cluster weight reads and the proposal writes.
+    // Algorithmic bytes of one affinity+decode pass over class c, counting
+    // the work done (profiling only; measured by role_work_kernel): per
+    // processed vertex offsets, list, cluster[v]/cluster weight reads and the
+    // proposal writes; per edge of a processed vertex its neighbour, edge
+    // weight and cluster gather (none at round 0); a skipped vertex reads its
+    // cluster and writes an empty proposal.
+    u64 work[kClasses][3] = {};
     auto affinity_bytes = [&](int c, bool identity) {
-        const double v = cnt[c], e = static_cast<double>(class_edges[c]);
-        return v * (2 * sizeof(O) + 4 + 4 + 8 + 4 + 8 + 4 + 8) + e * (4 + (ew ? sizeof(W) : 0) + (identity ? 0 : 4));
+        const double v = static_cast<double>(work[c][0]), e = static_cast<double>(work[c][1]);
+        return v * (2 * sizeof(O) + 4 + 4 + 8 + 4 + 8 + 4 + 8) + (static_cast<double>(cnt[c]) - v) * 8 +
+               e * (4 + (ew ? sizeof(W) : 0) + (identity ? 0 : 4));
     };
     auto affinity = [&](const RoundParams& p) {
         if (d.prof) {
+            Buf<u64> cw_dev(d, 3 * kClasses);
+            cw_dev.zero(d);
+            for (int c = 1; c < kClasses; ++c)
+                if (cnt[c])
+                    launch(d, "role_work_kernel", role_work_kernel<O>, stride_grid(d, cnt[c]), kThreads, 0,
+                           static_cast<i64>(cnt[c]), class_list(c), off, clusters, p, cw_dev.get() + 3 * c);
+            fetch(d, &work[0][0], cw_dev.get(), 3 * kClasses);
             d.prof_bytes("affinity_small_kernel", affinity_bytes(1, p.identity) + affinity_bytes(2, p.identity));
-            d.prof_bytes("affinity_warp_hash_kernel", affinity_bytes(3, p.identity));
-            d.prof_bytes("affinity_block_hash_kernel", affinity_bytes(4, p.identity));
-
+            if (!(p.identity && direct_ok)) {   // the direct kernels of identity rounds carry no model
+                d.prof_bytes("affinity_warp_hash_kernel", affinity_bytes(3, p.identity));
+                d.prof_bytes("affinity_block_hash_kernel", affinity_bytes(4, p.identity));
+            }
         }
         if (cnt[1])
             launch(d, "affinity_small_kernel", affinity_small_kernel<8, O, W>, blocks_for(static_cast<i64>(cnt[1]) * 8, kThreads), kThreads, 0, 
@@ -392,11 +404,14 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
             launch(d, "affinity_block_hash_kernel", affinity_block_hash_kernel<O, W>, static_cast<int>(cnt[4]), kThreads, kLargeSlots * 12, 
                 cnt[4], class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
         if (cnt[5]) {
-            d.prof_bytes("hub_insert_kernel", static_cast<double>(class_edges[5]) * (4 + 4 + (ew ? sizeof(W) : 0)) +
+            // chunk records of all hubs; neighbour, weight and cluster of
+            // each edge of the hubs that are not skipped; the slots of their
+            // tables for the candidate pass
+            d.prof_bytes("hub_insert_kernel", static_cast<double>(work[5][1]) * (4 + 4 + (ew ? sizeof(W) : 0)) +
                                                   static_cast<double>(hubs.chunks) * sizeof(Chunk));
             auto hub_tables = [&](auto* table) {
                 using S = std::remove_pointer_t<decltype(table)>;
-                d.prof_bytes("hub_candidates_kernel", static_cast<double>(table_total) * sizeof(S));
+                d.prof_bytes("hub_candidates_kernel", static_cast<double>(work[5][2]) * sizeof(S));
                 launch(d, "hub_insert_kernel", hub_insert_kernel<O, W, S>, static_cast<int>(hubs.chunks), kThreads, 0,
                        hubs.chunk.get(), nbr, ew, clusters, p, w.table_off.get(), table, d.err);
                 launch(d, "hub_candidates_kernel", hub_candidates_kernel<W, S>,
