@@ -81,6 +81,11 @@ struct Device {
     int device = 0;
     cudaStream_t stream = nullptr;
     int sms = 148;
+    // Contexts expected to run at once on the device (a server's slots): the
+    // grid-stride kernels of this context take at most 1/share of the
+    // device's block slots, so kernels of the other contexts fit beside them.
+    int share = 1;
+    int grid_limit(int per_sm) const { return std::max(sms / 2, sms * per_sm / std::max(1, share)); }
     u32* err = nullptr;         // device error word
     void* pinned = nullptr;     // small pinned host staging area
     static constexpr size_t kPinnedBytes = 1 << 16;

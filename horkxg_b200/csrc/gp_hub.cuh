@@ -153,10 +153,11 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
     const i64 t0 = table_off[ch.hub];
     const u32 size = static_cast<u32>(table_off[ch.hub + 1] - t0);
     S* slots = table + t0;
-    for (i64 base = ch.begin; base < ch.end; base += kThreads) {
-        const i64 e = base + threadIdx.x;
-        i32 c = -1;
-        u64 w = 0;
+    // The next edge's cluster is gathered before the current insert, so its
+    // load latency overlaps the CAS round trip.
+    auto gather = [&](i64 e, i32& c, u64& w) {
+        c = -1;
+        w = 0;
         if (e < ch.end) {
             const i32 u = nbr[e];
             if (u != ch.v) {
@@ -164,6 +165,14 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
                 w = static_cast<u64>(weight_at(ew, e));
             }
         }
+    };
+    i32 c_next;
+    u64 w_next;
+    gather(ch.begin + threadIdx.x, c_next, w_next);
+    for (i64 base = ch.begin; base < ch.end; base += kThreads) {
+        const i32 c = c_next;
+        const u64 w = w_next;
+        gather(base + kThreads + threadIdx.x, c_next, w_next);
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         u64 sum = 0;
         if (ew == nullptr) {
@@ -387,8 +396,13 @@ __global__ void __launch_bounds__(kThreads) hub_apply_kernel(i64 nchunks, const 
         if (mine < nchunks && flags[chunks[mine].v]) todo[atomicAdd(&ntodo, 1)] = static_cast<int>(threadIdx.x);
         __syncthreads();
         const int count = ntodo;
+        if (threadIdx.x == 0 && count)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->hub_chunks), static_cast<unsigned long long>(count));
         for (int j = 0; j < count; ++j) {
             const Chunk ch = chunks[base + static_cast<i64>(todo[j]) * stride];
+            if (threadIdx.x == 0)
+                atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->hub_edges),
+                          static_cast<unsigned long long>(ch.end - ch.begin));
             const i32 v = ch.v;
             const i32 s = labels[v], t = targets[v];
             for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {

@@ -207,7 +207,7 @@ __global__ void sat_sum_kernel(i64 m, const W* w, u64* out) {
 }
 
 inline int stride_grid(Device& d, i64 items, int per_block = kThreads) {
-    return static_cast<int>(std::min<i64>(blocks_for(items, per_block), static_cast<i64>(d.sms) * 8));
+    return static_cast<int>(std::min<i64>(blocks_for(items, per_block), d.grid_limit(8)));
 }
 
 // ---------------------------------------------------------------------------
@@ -1087,11 +1087,11 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
                    kThreads, 0, w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache,
                    ctr, w.list.get());
             launch(d, "apply_big_rows_kernel", apply_big_rows_kernel<O, W, C>,
-                   static_cast<int>(std::min<i64>(std::max<i64>(bound, 1), static_cast<i64>(d.sms) * 4)), kThreads, 0,
+                   static_cast<int>(std::min<i64>(std::max<i64>(bound, 1), d.grid_limit(4))), kThreads, 0,
                    w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
             if (hubs.count)
                 launch(d, "hub_apply_kernel", hub_apply_kernel<W, C>,
-                       static_cast<int>(std::min<i64>(hubs.chunks, static_cast<i64>(d.sms) * 8)), kThreads, 0,
+                       static_cast<int>(std::min<i64>(hubs.chunks, d.grid_limit(8))), kThreads, 0,
                        hubs.chunks, hubs.chunk.get(), nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
         }
         launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, bound), kThreads, 0, w.movers.get(), ctr, labels,
@@ -1111,6 +1111,12 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
                                                        static_cast<double>(h.c.walked_degree) * per_edge);
             d.prof_bytes("apply_big_rows_kernel",
                          static_cast<double>(h.c.big) * per_mover + static_cast<double>(h.c.big_degree) * per_edge);
+            // every chunk record and the mover flag of its hub; the edges of
+            // the moving hubs' chunks
+            if (hubs.count)
+                d.prof_bytes("hub_apply_kernel", static_cast<double>(hubs.chunks) * (sizeof(Chunk) + 1) +
+                                                     static_cast<double>(h.c.hub_chunks) * 8 +
+                                                     static_cast<double>(h.c.hub_edges) * per_edge);
         }
         if (rebuild) {
             current_cut = undirected_cut(d, g, labels, w.scratch.get());
@@ -1825,6 +1831,12 @@ void gp_ctx_destroy(gp_ctx* ctx) {
 }
 
 const char* gp_ctx_error(const gp_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+gp_status gp_ctx_set_device_share(gp_ctx* ctx, int share) {
+    if (!ctx || share < 1) return GP_EINVAL;
+    ctx->dev.share = share;
+    return GP_OK;
+}
 
 gp_status gp_ctx_set_sync_mode(gp_ctx* ctx, int blocking) {
     if (!ctx) return GP_EINVAL;

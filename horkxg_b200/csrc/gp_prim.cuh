@@ -363,7 +363,7 @@ void radix_sort(Device& d, K* keys, V* vals, K* keys_alt, V* vals_alt, i64 n, in
         return;
     }
     const int grid = static_cast<int>(std::min<i64>(std::max<i64>(1, (n + kSortTile - 1) / kSortTile),
-                                                    static_cast<i64>(d.sms) * 4));
+                                                    static_cast<i64>(d.grid_limit(4))));
     Buf<u32> hist(d, static_cast<size_t>(kRadix) * grid);
     Buf<i64> offs(d, static_cast<size_t>(kRadix) * grid);
     K* src_k = keys;

@@ -30,6 +30,8 @@ struct RefineCounters {
     i64 big;              // movers of degree > kSplitDegree handed to apply_big_rows_kernel
     i64 big_degree;       // their degree sum
     i64 walked_degree;    // edges apply_cache_cut_kernel walked itself
+    i64 hub_edges;        // edges of moving hubs walked by hub_apply_kernel
+    i64 hub_chunks;       // their chunks
 };
 
 // Per-vertex proposal record written by the LP pass: the priority filter

@@ -197,6 +197,7 @@ gp_status gp_server_create(int device, int32_t slots, uint64_t memory_budget, gp
             *out = nullptr;
             return st;
         }
+        gp_ctx_set_device_share(c, slots);
         s->slots.push_back(c);
     }
     for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker, s.get(), i);

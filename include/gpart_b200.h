@@ -205,6 +205,11 @@ uint64_t gp_sync_count(const gp_ctx* ctx);
  * done, which frees the core for other host threads when many contexts run
  * at once (the server's slots). */
 gp_status gp_ctx_set_sync_mode(gp_ctx* ctx, int blocking);
+/* Number of contexts expected to run at once on the device (default 1).
+ * The context's grid-stride kernels then take at most about 1/share of the
+ * device's block slots, so that kernels of other contexts run beside them;
+ * results do not depend on it.  The server sets it to its slot count. */
+gp_status gp_ctx_set_device_share(gp_ctx* ctx, int share);
 
 /* Spectral initial partition that allocates no device memory.
  *

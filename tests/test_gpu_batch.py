@@ -121,6 +121,16 @@ def test_blocking_sync_mode_same_labels(ctx):
     assert np.array_equal(la, lb) and ra.cut == rb.cut
 
 
+def test_device_share_same_labels(ctx):
+    """Smaller grids for contexts that share the device change no result."""
+    off, nbr = graphs.rmat_csr(14, 16, 8)
+    la, ra = alone(ctx, off, nbr, 16)
+    with hb.Context(0) as c:
+        c.set_device_share(8)
+        lb, rb = alone(c, off, nbr, 16)
+    assert np.array_equal(la, lb) and ra.cut == rb.cut
+
+
 @pytest.mark.parametrize("make,k", [(lambda: graphs.rmat_csr(16, 16, 1), 32), (lambda: graphs.grid2d_csr(300, 300), 4),
                                     (lambda: graphs.rgg_csr(100000, 10.0, 3), 16)])
 def test_footprint_bounds_measured_peak(make, k):
