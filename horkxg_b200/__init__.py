@@ -73,7 +73,7 @@ class RefineStats(ctypes.Structure):
 EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_error", "gp_partition_capacity",
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
-           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
+           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
            "gp_initial_partition_static", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
            "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
            "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
@@ -113,6 +113,7 @@ def lib() -> ctypes.CDLL:
         L.gp_sync_count.restype = ctypes.c_uint64
         L.gp_ctx_set_sync_mode.argtypes = [vp, i32]
         L.gp_ctx_set_device_share.argtypes = [vp, i32]
+        L.gp_ctx_set_small_diffusion.argtypes = [vp, i32]
         L.gp_ctx_stream.argtypes = [vp]
         L.gp_ctx_stream.restype = vp
         L.gp_profile_enable.argtypes = [vp, i32]
@@ -352,6 +353,10 @@ class Context:
     @property
     def syncs(self) -> int:
         return int(lib().gp_sync_count(self._h))
+
+    def set_small_diffusion(self, enable: bool):
+        """One-block diffusion for small coarsest graphs (same values)."""
+        self._check(lib().gp_ctx_set_small_diffusion(self._h, int(enable)))
 
     def set_device_share(self, share: int):
         """Contexts expected to run at once on the device (grid sizing only)."""

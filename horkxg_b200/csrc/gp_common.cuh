@@ -85,6 +85,9 @@ struct Device {
     // grid-stride kernels of this context take at most 1/share of the
     // device's block slots, so kernels of the other contexts fit beside them.
     int share = 1;
+    // Small coarsest graphs take the one-block diffusion (same values as the
+    // cooperative kernel); off only to compare the two.
+    bool small_diffusion = true;
     int grid_limit(int per_sm) const { return std::max(sms / 2, sms * per_sm / std::max(1, share)); }
     u32* err = nullptr;         // device error word
     void* pinned = nullptr;     // small pinned host staging area

@@ -16,6 +16,8 @@
 // checked against the FP64 oracle within 1e-5 relative L2.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "gp_prim.cuh"
 
 namespace gp {
@@ -31,6 +33,7 @@ struct InitTask {
 };
 
 struct Moments { float mass, sum, squares; };
+struct alignas(16) Moments4 { float mass, sum, squares, pad; };   // one 16-byte store
 
 // Bounded grid barrier for cooperative launches: gives up after ~2^24 polls
 // and records kErrTimeout (the kernel then finishes with garbage values that
@@ -67,10 +70,13 @@ struct NormShared {
 
 // Every block computes every task's (mean, scale) from the per-position
 // contributions in the same order: deterministic and identical everywhere.
+// Only the first kWarps warps take part, so blocks larger than kThreads get
+// the same result.
 // The tasks are reduced side by side: `wpt` warps per task, each warp over a
 // lane-strided slice with an xor-shuffle tree, then one thread per task adds
 // its warps' partials in warp order.
-__device__ void compute_norms(int tasks, const InitTask* task, const Moments* contrib, NormShared& sh) {
+template <typename Rec>
+__device__ void compute_norms(int tasks, const InitTask* task, const Rec* contrib, NormShared& sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int wpt = kWarps;
     while (wpt > 1 && tasks * wpt > kWarps) wpt >>= 1;
@@ -79,10 +85,10 @@ __device__ void compute_norms(int tasks, const InitTask* task, const Moments* co
         const int t = t0 + warp / wpt;
         const int part = warp % wpt;
         float m = 0.f, s = 0.f, q = 0.f;
-        if (t < tasks) {
+        if (warp < kWarps && t < tasks) {
             const i32 b = task[t].begin, c = task[t].count;
             for (i32 i = part * 32 + lane; i < c; i += wpt * 32) {
-                const Moments x = contrib[b + i];
+                const Rec x = contrib[b + i];
                 m += x.mass; s += x.sum; q += x.squares;
             }
 #pragma unroll
@@ -92,7 +98,7 @@ __device__ void compute_norms(int tasks, const InitTask* task, const Moments* co
                 q += __shfl_xor_sync(0xffffffffu, q, o);
             }
         }
-        if (lane == 0) { sh.red[0][warp] = m; sh.red[1][warp] = s; sh.red[2][warp] = q; }
+        if (lane == 0 && warp < kWarps) { sh.red[0][warp] = m; sh.red[1][warp] = s; sh.red[2][warp] = q; }
         __syncthreads();
         if (threadIdx.x < per_round && t0 + static_cast<int>(threadIdx.x) < tasks) {
             float M = 0.f, S = 0.f, Q = 0.f;
@@ -238,6 +244,196 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
         const u32 ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
         key[p] = (static_cast<u64>(ord) << 32) | static_cast<u32>(v);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Small coarsest graphs: the same diffusion in ONE thread-block cluster of
+// kSmallDiffCluster blocks (1024 threads each), every per-vertex and
+// per-position array in shared memory and the hardware cluster barrier in
+// place of the grid barrier (no cooperative launch, no polling).  Each block
+// owns the positions p with p % cluster size == its rank.  The new values of
+// its rows are written into every block's shared memory (distributed shared
+// memory), their moment contributions into block 0's only; block 0 runs
+// compute_norms and sends the per-task mean and scale to the others.  It
+// computes exactly the values of diffusion_kernel, operation for operation:
+// * rows of more than 32 edges are summed by a warp with the same row_sum and
+//   warp_sum;
+// * rows of at most 32 edges are summed by one thread: in row_sum (stride 32)
+//   each lane then holds at most one edge, so the thread forms the 32 lane
+//   values and adds them in the butterfly order of warp_sum;
+// * the moments use compute_norms on the first kWarps warps.
+// Rows of more than kHeavyRow edges (block sums) are not taken: the host
+// sends such graphs to diffusion_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kSmallDiffThreads = 1024;
+constexpr int kSmallDiffWarps = kSmallDiffThreads / 32;
+constexpr int kSmallDiffCluster = 8;       // portable cluster size
+constexpr i32 kSmallDiffN = 4096;          // positions (= vertices of the coarsest graph)
+constexpr i64 kSmallDiffM = 65536;         // edges
+constexpr i32 kThreadRowMax = 32;          // rows summed by a single thread
+
+// Lane 0's result of warp_sum over the 32 lane values lane(l), l = 0..31.
+template <typename L>
+__device__ __forceinline__ float butterfly_sum(L lane) {
+    float r[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) r[l] = lane(l);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+#pragma unroll
+        for (int l = 0; l < o; ++l) r[l] = r[l] + r[l + o];
+    }
+    return r[0];
+}
+
+inline size_t small_diffusion_smem(i32 n) {
+    // moment records (per position; used in block 0), x, y, degree
+    // (vertex-indexed floats), labels, position records {vertex,
+    // degree << 8 | task} and the list of rows summed by warps
+    return static_cast<size_t>(n) * (sizeof(Moments4) + 3 * sizeof(float) + 4 * sizeof(i32));
+}
+
+template <typename O, typename W>
+__global__ void __cluster_dims__(kSmallDiffCluster, 1, 1) __launch_bounds__(kSmallDiffThreads) diffusion_small_kernel(
+    int tasks, const InitTask* __restrict__ task, const i32* __restrict__ task_of_pos, i32 positions,
+    const i32* __restrict__ order, const i32* __restrict__ labels_g, const O* __restrict__ off,
+    const i32* __restrict__ nbr, const W* __restrict__ ew, u32 seed, int steps, float* x_out, u64* key) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = static_cast<int>(cluster.block_rank());
+    const int cs = static_cast<int>(cluster.num_blocks());
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const i32 n = positions;
+    Moments4* contrib = reinterpret_cast<Moments4*>(smem_raw);
+    float* xa = reinterpret_cast<float*>(contrib + n);
+    float* xb = xa + n;
+    float* deg = xb + n;
+    i32* labels = reinterpret_cast<i32*>(deg + n);
+    i32* pv = labels + n;
+    i32* pdt = pv + n;
+    i32* heavy = pdt + n;
+    __shared__ NormShared sh;
+    __shared__ float norm_mean[kMaxInitTasks], norm_scale[kMaxInitTasks];
+    __shared__ int nheavy;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) nheavy = 0;
+    for (i32 v = threadIdx.x; v < n; v += kSmallDiffThreads) labels[v] = labels_g[v];
+    __syncthreads();
+    const i32 first = rank + cs * static_cast<i32>(threadIdx.x);
+    const i32 stride = cs * kSmallDiffThreads;
+    for (i32 p = first; p < n; p += stride) {
+        const i32 t = task_of_pos[p];
+        const i32 v = order[p];
+        const i32 dg = static_cast<i32>(off[v + 1] - off[v]);
+        pv[p] = v;
+        pdt[p] = t < 0 ? -1 : (dg << 8) | t;
+        if (t >= 0 && dg > kThreadRowMax) heavy[atomicAdd(&nheavy, 1)] = p;
+    }
+    cluster.sync();   // every block has started: its shared memory may be written
+    const int nh = nheavy;
+    Moments4* contrib0 = cluster.map_shared_rank(contrib, 0);
+    // a row's new value goes to every block, its moment record to block 0
+    auto put = [&](float* xlocal, i32 p, i32 v, float mass, float a) {
+        for (int r = 0; r < cs; ++r) cluster.map_shared_rank(xlocal, r)[v] = a;
+        contrib0[p] = Moments4{mass, mass * a, mass * a * a, 0.f};
+    };
+    auto start_row = [&](i32 p, float d) {
+        const i32 v = pv[p];
+        const i32 group = task[pdt[p] & 0xff].first_part;
+        const u32 h = mix32(static_cast<u32>(v) ^ (seed ^ static_cast<u32>(group)));
+        const float a = static_cast<float>(static_cast<double>(h) / 4294967296.0 - 0.5);
+        deg[v] = d;
+        put(xa, p, v, d > 0.f ? d : 1.f, a);
+    };
+    // row sum of f over the group, as diffusion_kernel forms it: lane l of
+    // row_sum holds edge l alone, a0 = 0 + w * f(u) if u is in the group,
+    // and returns (a0 + a1) + (a2 + a3) with a1 = a2 = a3 = 0
+    auto sum_thread = [&](i32 p, auto f) {
+        const i32 v = pv[p];
+        const i64 b = static_cast<i64>(off[v]);
+        const int dg = pdt[p] >> 8;
+        const i32 group = task[pdt[p] & 0xff].first_part;
+        return butterfly_sum([&](int l) {
+            float a0 = 0.f;
+            if (l < dg) {
+                const i32 u = nbr[b + l];
+                if (labels[u] == group) a0 += static_cast<float>(weight_at(ew, b + l)) * f(u);
+            }
+            const float a1 = 0.f, a2 = 0.f, a3 = 0.f;
+            return (a0 + a1) + (a2 + a3);
+        });
+    };
+    auto sum_warp = [&](i32 p, auto f) {
+        const i32 v = pv[p];
+        const i64 b = static_cast<i64>(off[v]);
+        const i64 e = b + (pdt[p] >> 8);
+        const i32 group = task[pdt[p] & 0xff].first_part;
+        return warp_sum(row_sum<O, W>(b, e, lane, 32, nbr, labels, group, ew, f));
+    };
+    for (i32 p = first; p < n; p += stride)
+        if (pdt[p] >= 0 && (pdt[p] >> 8) <= kThreadRowMax) start_row(p, sum_thread(p, One{}));
+    for (int h = warp; h < nh; h += kSmallDiffWarps) {
+        const float d = sum_warp(heavy[h], One{});
+        if (lane == 0) start_row(heavy[h], d);
+    }
+    float* x = xa;
+    float* y = xb;
+    for (int it = 0; it <= steps; ++it) {
+        cluster.sync();                       // all records of the step are in block 0
+        if (rank == 0) {
+            compute_norms(tasks, task, contrib, sh);
+            if (threadIdx.x < static_cast<unsigned>(tasks))
+                for (int r = 0; r < cs; ++r) {
+                    cluster.map_shared_rank(norm_mean, r)[threadIdx.x] = sh.mean[threadIdx.x];
+                    cluster.map_shared_rank(norm_scale, r)[threadIdx.x] = sh.scale[threadIdx.x];
+                }
+        }
+        cluster.sync();                       // mean and scale are everywhere
+        if (it == steps) break;
+        auto step_row = [&](i32 p, float s) {
+            const i32 v = pv[p];
+            const int t = pdt[p] & 0xff;
+            const float d = deg[v];
+            const float xv = (x[v] - norm_mean[t]) * norm_scale[t];
+            const float a = d > 0.f ? 0.5f * (xv + s / d) : xv;
+            put(y, p, v, d > 0.f ? d : 1.f, a);
+        };
+        for (i32 p = first; p < n; p += stride) {
+            if (pdt[p] < 0 || (pdt[p] >> 8) > kThreadRowMax) continue;
+            const int t = pdt[p] & 0xff;
+            step_row(p, sum_thread(p, Normalised{x, norm_mean[t], norm_scale[t]}));
+        }
+        for (int h = warp; h < nh; h += kSmallDiffWarps) {
+            const i32 p = heavy[h];
+            const int t = pdt[p] & 0xff;
+            const float s = sum_warp(p, Normalised{x, norm_mean[t], norm_scale[t]});
+            if (lane == 0) step_row(p, s);
+        }
+        float* tmp = x; x = y; y = tmp;
+    }
+    // no shared memory of another block is touched after the last cluster.sync
+    for (i32 p = first; p < n; p += stride) {
+        if (pdt[p] < 0) continue;
+        const int t = pdt[p] & 0xff;
+        const i32 v = pv[p];
+        float a = (x[v] - norm_mean[t]) * norm_scale[t];
+        if (a == 0.f) a = 0.f;
+        if (x_out) x_out[v] = a;
+        const u32 bits = __float_as_uint(a);
+        const u32 ord = (bits & 0x80000000u) ? ~bits : (bits | 0x80000000u);
+        key[p] = (static_cast<u64>(ord) << 32) | static_cast<u32>(v);
+    }
+}
+
+template <typename O>
+__global__ void max_degree_kernel(i64 n, const O* off, u64* out) {
+    u64 m = 0;
+    for (i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const u64 dg = static_cast<u64>(off[v + 1] - off[v]);
+        m = dg > m ? dg : m;
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0 && m) atomic_max_u64(out, m);
 }
 
 __global__ void task_positions_kernel(int tasks, const InitTask* task, i32* task_of_pos) {

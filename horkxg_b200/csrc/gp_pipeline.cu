@@ -824,9 +824,21 @@ std::vector<DepthPlan> plan_tasks(int parts) {
 template <typename T>
 void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask* tasks, const i32* task_of_pos,
                       i32 positions, const i32* order, const i32* labels, u32 seed, int steps, float* deg, float* xa,
-                      float* xb, Moments* contrib, float* x_out, u64* key, u32* bar) {
+                      float* xb, Moments* contrib, float* x_out, u64* key, u32* bar, i64 max_degree = -1) {
     using O = typename T::O;
     using W = typename T::W;
+    // Small graphs (max_degree known, every row within a warp's reach): one
+    // thread-block cluster, same values, no grid barriers.
+    if (d.small_diffusion && max_degree >= 0 && max_degree <= kHeavyRow && positions <= kSmallDiffN &&
+        g.m <= kSmallDiffM && positions == g.n) {
+        auto small = diffusion_small_kernel<O, W>;
+        const size_t smem = small_diffusion_smem(positions);
+        GP_CUDA(cudaFuncSetAttribute(small, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        launch(d, "diffusion_small_kernel", small, kSmallDiffCluster, kSmallDiffThreads, smem, ntasks, tasks, task_of_pos, positions,
+               order, labels, g.off.get(), g.nbr.get(), g.ewp(), seed, steps, x_out, key);
+        GP_LAUNCH();
+        return;
+    }
     auto kernel = diffusion_kernel<O, W>;
     int per_sm = 0;
     GP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
@@ -867,10 +879,13 @@ void initial_partition(Device& d, const DGraph<T>& g, int parts, double ratio, u
     sc.zero(d);
     launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, n), kThreads, 0, n, g.vwp(), sc.get());
     launch(d, "sat_sum_kernel", sat_sum_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), sc.get() + 2);
+    launch(d, "max_degree_kernel", max_degree_kernel<typename T::O>, stride_grid(d, n), kThreads, 0, n64, g.off.get(),
+           sc.get() + 3);
     GP_LAUNCH();
-    u64 st[3];
-    fetch(d, st, sc.get(), 3);
+    u64 st[4];
+    fetch(d, st, sc.get(), 4);
     const u64 total = st[0], maxw = st[1], edge_total = st[2];
+    const i64 max_degree = static_cast<i64>(st[3]);
     if (!total || total == ~0ULL || edge_total == ~0ULL)
         fail(GP_EOVERFLOW, "GPU initializer weight accumulation overflow");
     const u64 capacity = partition_capacity(total, parts, ratio);
@@ -898,7 +913,7 @@ void initial_partition(Device& d, const DGraph<T>& g, int parts, double ratio, u
         launch(d, "task_positions_kernel", task_positions_kernel, nt, kThreads, 0, nt, dtasks[dpt].get(), task_of_pos.get());
         GP_LAUNCH();
         launch_diffusion(d, g, nt, dtasks[dpt].get(), task_of_pos.get(), n, order.get(), labels.get(), seed, 64,
-                         deg.get(), xa.get(), xb.get(), contrib.get(), nullptr, key.get(), bar.get());
+                         deg.get(), xa.get(), xb.get(), contrib.get(), nullptr, key.get(), bar.get(), max_degree);
         launch(d, "task_sort_kernel", task_sort_kernel, nt, kThreads, 0, nt, dtasks[dpt].get(), key.get(), key_alt.get(), order.get());
         InitTask* next = dpt + 1 < depths.size() ? dtasks[dpt + 1].get() : nullptr;
         launch(d, "task_split_kernel", task_split_kernel<W>, nt, kThreads, 0, nt, dtasks[dpt].get(), next, order.get(), g.vwp(), capacity,
@@ -1838,6 +1853,12 @@ gp_status gp_ctx_set_device_share(gp_ctx* ctx, int share) {
     return GP_OK;
 }
 
+gp_status gp_ctx_set_small_diffusion(gp_ctx* ctx, int enable) {
+    if (!ctx) return GP_EINVAL;
+    ctx->dev.small_diffusion = enable != 0;
+    return GP_OK;
+}
+
 gp_status gp_ctx_set_sync_mode(gp_ctx* ctx, int blocking) {
     if (!ctx) return GP_EINVAL;
     return guarded(ctx, [&] {
@@ -2202,8 +2223,15 @@ gp_status gp_diffusion(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels
             gp::Buf<gp::u64> key(d, n);
             gp::Buf<gp::u32> bar(d, 2);
             xo.zero(d);
+            gp::Buf<gp::u64> md(d, 1);
+            md.zero(d);
+            gp::launch(d, "max_degree_kernel", gp::max_degree_kernel<typename T::O>, gp::stride_grid(d, g.n), gp::kThreads,
+                       0, g.n, g.off.get(), md.get());
+            gp::u64 max_degree = 0;
+            gp::fetch(d, &max_degree, md.get(), 1);
             gp::launch_diffusion<T>(d, g, 1, dt.get(), top.get(), n, order.get(), dl.get(), seed, steps, deg.get(),
-                                    xa.get(), xb.get(), contrib.get(), xo.get(), key.get(), bar.get());
+                                    xa.get(), xb.get(), contrib.get(), xo.get(), key.get(), bar.get(),
+                                    static_cast<gp::i64>(max_degree));
             d.check_errors();
             gp::to_host(d, x, xo.get(), static_cast<size_t>(n));
             d.sync();

@@ -167,6 +167,42 @@ def test_diffusion_subgroup_and_coarse_level(ctx):
         assert rel_l2(x, ref) < DIFFUSION_TOL
 
 
+@pytest.mark.parametrize("name", ["grid2d_64", "rmat12", "cycle_hub_4096"])
+def test_small_diffusion_equals_grid_kernel(ctx, name):
+    """The one-block diffusion of small graphs computes the cooperative
+    kernel's values bit for bit: vectors, initial partition and the whole
+    deterministic partition."""
+    off, idx, g = file_graph(name)
+    n = len(off) - 1
+    with hb.Context(0) as grid:
+        grid.set_small_diffusion(False)
+        for group, seed, labels in ((0, 0, np.zeros(n, np.int32)),
+                                    (16, 7, np.where(np.arange(n) % 3 == 0, 16, 0).astype(np.int32))):
+            a = ctx.diffusion(g, labels, group, seed, 64)
+            b = grid.diffusion(g, labels, group, seed, 64)
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        for k in (2, 8, 32):
+            assert np.array_equal(ctx.initial_partition(g, k, 1.03, 3), grid.initial_partition(g, k, 1.03, 3))
+        if name != "cycle_hub_4096":   # not a symmetric CSR: diffusion fixture only
+            la, ra = ctx.partition(g, parts=8, deterministic=1)
+            lb, rb = grid.partition(g, parts=8, deterministic=1)
+            assert np.array_equal(la, lb) and ra.cut == rb.cut
+
+
+def test_small_diffusion_on_coarse_level(ctx):
+    off, idx, g = file_graph("rmat14")
+    coff, cnbr, cew, cvw, _ = ctx.coarsen(g, parts=32)[-1]
+    n = len(cvw)
+    assert n <= 4096
+    cg = hb.HostGraph(coff, cnbr, cew, cvw, width=hb.STANDARD, index64=False)
+    labels = np.where(np.arange(n) % 3 == 0, 16, 0).astype(np.int32)
+    with hb.Context(0) as grid:
+        grid.set_small_diffusion(False)
+        a = ctx.diffusion(cg, labels, 16, 7, 64)
+        b = grid.diffusion(cg, labels, 16, 7, 64)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 # --- initial partition (tests/test_initial_partition_gpu.cu:13-100)
 def test_initial_partition_fixtures(ctx):
     rows = [[u for u in range(8) if u != v and u // 4 == v // 4] for v in range(8)]
