@@ -247,8 +247,9 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Small coarsest graphs: the same diffusion in ONE thread-block cluster of
-// kSmallDiffCluster blocks (1024 threads each), every per-vertex and
+// Small coarsest graphs: the same diffusion in ONE thread-block cluster of up
+// to kSmallDiffCluster blocks (1024 threads each, one block per 1024
+// positions, so each thread owns at most one row), every per-vertex and
 // per-position array in shared memory and the hardware cluster barrier in
 // place of the grid barrier (no cooperative launch, no polling).  Each block
 // owns the positions p with p % cluster size == its rank.  The new values of
@@ -267,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
 // ---------------------------------------------------------------------------
 constexpr int kSmallDiffThreads = 1024;
 constexpr int kSmallDiffWarps = kSmallDiffThreads / 32;
-constexpr int kSmallDiffCluster = 8;       // portable cluster size
+constexpr int kSmallDiffCluster = 8;       // largest cluster (portable size)
 constexpr i32 kSmallDiffN = 4096;          // positions (= vertices of the coarsest graph)
 constexpr i64 kSmallDiffM = 65536;         // edges
 constexpr i32 kThreadRowMax = 32;          // rows summed by a single thread
@@ -294,7 +295,7 @@ inline size_t small_diffusion_smem(i32 n) {
 }
 
 template <typename O, typename W>
-__global__ void __cluster_dims__(kSmallDiffCluster, 1, 1) __launch_bounds__(kSmallDiffThreads) diffusion_small_kernel(
+__global__ void __launch_bounds__(kSmallDiffThreads) diffusion_small_kernel(
     int tasks, const InitTask* __restrict__ task, const i32* __restrict__ task_of_pos, i32 positions,
     const i32* __restrict__ order, const i32* __restrict__ labels_g, const O* __restrict__ off,
     const i32* __restrict__ nbr, const W* __restrict__ ew, u32 seed, int steps, float* x_out, u64* key) {

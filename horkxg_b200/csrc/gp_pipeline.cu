@@ -834,9 +834,33 @@ void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask*
         auto small = diffusion_small_kernel<O, W>;
         const size_t smem = small_diffusion_smem(positions);
         GP_CUDA(cudaFuncSetAttribute(small, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        launch(d, "diffusion_small_kernel", small, kSmallDiffCluster, kSmallDiffThreads, smem, ntasks, tasks, task_of_pos, positions,
-               order, labels, g.off.get(), g.nbr.get(), g.ewp(), seed, steps, x_out, key);
-        GP_LAUNCH();
+        int cs = 1;   // one block per 1024 positions, a power of two
+        while (cs < kSmallDiffCluster && cs * kSmallDiffThreads < positions) cs *= 2;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(kSmallDiffThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = d.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaEvent_t ev0 = nullptr;
+        if (d.prof) { ev0 = d.event(); GP_CUDA(cudaEventRecord(ev0, d.stream)); }
+        const O* off = g.off.get();
+        GP_CUDA(cudaLaunchKernelEx(&cfg, small, ntasks, tasks, task_of_pos, positions, order, labels, off,
+                                   g.nbr.get(), g.ewp(), seed, steps, x_out, key));
+        ++d.launches;
+        if (d.prof) {
+            cudaEvent_t ev1 = d.event();
+            GP_CUDA(cudaEventRecord(ev1, d.stream));
+            auto& e = d.prof_table["diffusion_small_kernel"];
+            e.pending.push_back({ev0, ev1});
+            ++e.launches;
+        }
         return;
     }
     auto kernel = diffusion_kernel<O, W>;

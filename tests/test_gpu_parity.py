@@ -189,6 +189,25 @@ def test_small_diffusion_equals_grid_kernel(ctx, name):
             assert np.array_equal(la, lb) and ra.cut == rb.cut
 
 
+@pytest.mark.parametrize("nx,ny", [(20, 20), (40, 40), (50, 60)])
+def test_small_diffusion_cluster_sizes(ctx, nx, ny):
+    """One, two and four blocks per cluster give the cooperative kernel's
+    values too."""
+    from horkxg_b200 import graphs
+    off, nbr = graphs.grid2d_csr(nx, ny)
+    g = hb.HostGraph(off, nbr)
+    n = len(off) - 1
+    labels = np.where(np.arange(n) % 5 == 0, 3, 1).astype(np.int32)
+    with hb.Context(0) as grid:
+        grid.set_small_diffusion(False)
+        for group, seed in ((1, 0), (3, 9)):
+            a = ctx.diffusion(g, labels, group, seed, 64)
+            b = grid.diffusion(g, labels, group, seed, 64)
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        for k in (2, 16):
+            assert np.array_equal(ctx.initial_partition(g, k, 1.03, 5), grid.initial_partition(g, k, 1.03, 5))
+
+
 def test_small_diffusion_on_coarse_level(ctx):
     off, idx, g = file_graph("rmat14")
     coff, cnbr, cew, cvw, _ = ctx.coarsen(g, parts=32)[-1]
