@@ -833,7 +833,10 @@ void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask*
         g.m <= kSmallDiffM && positions == g.n) {
         auto small = diffusion_small_kernel<O, W>;
         const size_t smem = small_diffusion_smem(positions);
-        GP_CUDA(cudaFuncSetAttribute(small, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        // the attribute is shared by every thread of the process (server
+        // slots launch concurrently): always the largest size, never lowered
+        GP_CUDA(cudaFuncSetAttribute(small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(small_diffusion_smem(kSmallDiffN))));
         int cs = 1;   // one block per 1024 positions, a power of two
         while (cs < kSmallDiffCluster && cs * kSmallDiffThreads < positions) cs *= 2;
         cudaLaunchConfig_t cfg{};
