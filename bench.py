@@ -267,7 +267,7 @@ def recount_ok(off, nbr, labels, cut) -> bool:
     return int(np.count_nonzero(labels[src] != labels[nbr])) == 2 * cut
 
 
-def run_batched(local: int, slots: int, passes: int = 3):
+def run_batched(local: int, slots: int, passes: int = 5):
     """Batched workload: 512 random geometric graphs (n log-uniform in
     [1e3, 1e6], mean degree 10, k uniform in {2,4,8,16,32}, seed 7) in one
     packed CSR in pinned host memory.  "plain" partitions them one by one on
