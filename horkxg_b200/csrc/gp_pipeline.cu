@@ -86,7 +86,11 @@ struct DGraph {
     mutable Hubs hubs;
     // rows free of duplicate neighbours: 1 yes, 0 no, -1 not yet checked
     mutable int unique_rows = -1;
+    // vertices of degree in (256, 2048] (the refinement's block-walked
+    // rows), from the degree classes of an aggregation; -1 unknown
+    mutable i64 mid_rows = -1;
 };
+static_assert(kSplitDegree == 256, "mid_rows counts SCLP degree class 4, (256, kHubDegree]");
 
 // known_count: the number of hub vertices when the caller already has it
 // (the degree classes of an aggregation); 0 skips the scans.
@@ -317,6 +321,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         w.edge_total_known = true;
     }
     const int sum32 = w.edge_total <= 0xffffffffULL ? 1 : 0;
+    g.mid_rows = static_cast<i64>(cnt[4]);
     const auto& hubs = hub_index(d, g, static_cast<i64>(cnt[5]));
     // hash-free affinity on identity rounds (rows without duplicates)
     const bool direct_ok = unique_rows(d, g);
@@ -1091,7 +1096,7 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         max_edge_weight = w.scratch.get() + 7;
     }
     struct Stats { RefineCounters c; u64 pw[32]; };
-    Buf<Stats> stats_dev(d, 1);
+    static_assert(sizeof(Stats) <= Device::kPinnedBytes, "stats fit the pinned staging buffer");
     auto build_cache = [&]() {
         launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr,
                ew, labels, k, cache);
@@ -1128,7 +1133,8 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
             launch(d, "apply_cache_cut_kernel", apply_cache_cut_kernel<O, W, C>, stride_grid(d, bound * 32),
                    kThreads, 0, w.movers.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache,
                    ctr, w.list.get());
-            launch(d, "apply_big_rows_kernel", apply_big_rows_kernel<O, W, C>,
+            if (g.mid_rows != 0)   // no row between kSplitDegree and the hub degree: nothing set aside
+                launch(d, "apply_big_rows_kernel", apply_big_rows_kernel<O, W, C>,
                    static_cast<int>(std::min<i64>(std::max<i64>(bound, 1), d.grid_limit(4))), kThreads, 0,
                    w.list.get(), ctr, off, nbr, ew, labels, w.targets.get(), w.flags.get(), k, cache, ctr);
             if (hubs.count)
@@ -1140,10 +1146,16 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
                w.targets.get(), vw, pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
         if (rebuild) build_cache();
         trace().mark(d, rebuild ? "refine.rebuild" : "refine.apply", c0.movers, c0.mover_degree);
-        GP_CUDA(cudaMemcpyAsync(&stats_dev.get()->c, ctr, sizeof(RefineCounters), cudaMemcpyDeviceToDevice, d.stream));
-        GP_CUDA(cudaMemcpyAsync(stats_dev.get()->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToDevice, d.stream));
+        // counters and part weights straight into the pinned staging buffer,
+        // one wait for both
         Stats h;
-        fetch(d, &h, stats_dev.get(), 1);
+        {
+            auto* staged = reinterpret_cast<Stats*>(d.pinned);
+            GP_CUDA(cudaMemcpyAsync(&staged->c, ctr, sizeof(RefineCounters), cudaMemcpyDeviceToHost, d.stream));
+            GP_CUDA(cudaMemcpyAsync(staged->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToHost, d.stream));
+            d.sync();
+            std::memcpy(&h, staged, sizeof(Stats));
+        }
         if (d.prof && !rebuild) {
             // per mover: offsets, label and target; per mover edge: neighbour,
             // weight, the neighbour's label and two read-modify-writes of the cache
@@ -1220,17 +1232,16 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         else ncand = n;
         const i64* dev_count = host_count ? nullptr : cand_count;
         const int cgrid = host_count ? blocks_for(std::max<i64>(ncand, 1), kThreads) : stride_grid(d, n);
+        w.counts.zero(d);   // bucket_scan_kernel leaves the counts zero for the next pass
         for (int it = 0; it < 2 * k + 4 && maximum() > cap; ++it) {
             ++st.admission_iterations;
             GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
-            w.counts.zero(d);
             launch(d, "rebalance_proposals_kernel", rebalance_proposals_kernel<C, W>, cgrid, kThreads, 0, ncand,
                    dev_count, w.cand.get(), cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(),
                    w.gpw.get(), w.bucket.get(), w.rank.get(), w.counts.get());
             GP_LAUNCH();
             if (deterministic) deterministic_ranks();
             launch(d, "bucket_scan_kernel", bucket_scan_kernel, k, kThreads, 0, w.counts.get(), w.offsets.get());
-            w.counts.zero(d);
             launch(d, "select_sources_kernel", select_sources_kernel<W>, cgrid, kThreads, 0, ncand, dev_count,
                    w.cand.get(),
                    w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, w.targets.get(), vw, deterministic ? 1 : 0,

@@ -511,8 +511,9 @@ __global__ void rebalance_proposals_kernel(i64 n, const i64* count, const i32* _
 }
 
 // balance_scan_buckets (src/refine_incremental.cuh:188-202): exclusive scan
-// of the 800 buckets of each part, block per part.
-__global__ void __launch_bounds__(kThreads) bucket_scan_kernel(const u64* counts, u64* offsets) {
+// of the 800 buckets of each part, block per part.  The counts are left
+// zero for the next ranking pass.
+__global__ void __launch_bounds__(kThreads) bucket_scan_kernel(u64* counts, u64* offsets) {
     __shared__ u64 sh[kWarps + 1];
     constexpr int kPer = (kBalWidth + kThreads - 1) / kThreads;   // 4
     u64 vals[kPer];
@@ -521,6 +522,7 @@ __global__ void __launch_bounds__(kThreads) bucket_scan_kernel(const u64* counts
     for (int i = 0; i < kPer; ++i) {
         const int b = threadIdx.x * kPer + i;
         vals[i] = b < kBalWidth ? counts[blockIdx.x * kBalWidth + b] : 0;
+        if (b < kBalWidth) counts[blockIdx.x * kBalWidth + b] = 0;
         local += vals[i];
     }
     u64 run = block_exclusive_sum(local, sh, static_cast<u64*>(nullptr));
