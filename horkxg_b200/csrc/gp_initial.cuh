@@ -248,8 +248,10 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
 
 // ---------------------------------------------------------------------------
 // Small coarsest graphs: the same diffusion in ONE thread-block cluster of up
-// to kSmallDiffCluster blocks (1024 threads each, one block per 1024
-// positions, so each thread owns at most one row), every per-vertex and
+// to kSmallDiffCluster blocks (1024 threads each; at least one block per 1024
+// positions, so each thread owns at most one row, and one per
+// kSmallDiffBlockEdges edges, for dense graphs whose rows go to warps), every
+// per-vertex and
 // per-position array in shared memory and the hardware cluster barrier in
 // place of the grid barrier (no cooperative launch, no polling).  Each block
 // owns the positions p with p % cluster size == its rank.  The new values of
@@ -268,9 +270,10 @@ __global__ void __launch_bounds__(kThreads) diffusion_kernel(
 // ---------------------------------------------------------------------------
 constexpr int kSmallDiffThreads = 1024;
 constexpr int kSmallDiffWarps = kSmallDiffThreads / 32;
-constexpr int kSmallDiffCluster = 8;       // largest cluster (portable size)
+constexpr int kSmallDiffCluster = 16;      // largest cluster (a non-portable size above 8)
 constexpr i32 kSmallDiffN = 4096;          // positions (= vertices of the coarsest graph)
-constexpr i64 kSmallDiffM = 65536;         // edges
+constexpr i64 kSmallDiffBlockEdges = 131072;                         // edges per block and step
+constexpr i64 kSmallDiffM = kSmallDiffCluster * kSmallDiffBlockEdges;   // edges
 constexpr i32 kThreadRowMax = 32;          // rows summed by a single thread
 
 // Lane 0's result of warp_sum over the 32 lane values lane(l), l = 0..31.

@@ -842,8 +842,11 @@ void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask*
         // slots launch concurrently): always the largest size, never lowered
         GP_CUDA(cudaFuncSetAttribute(small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(small_diffusion_smem(kSmallDiffN))));
-        int cs = 1;   // one block per 1024 positions, a power of two
-        while (cs < kSmallDiffCluster && cs * kSmallDiffThreads < positions) cs *= 2;
+        // a power of two: one block per 1024 positions and per
+        // kSmallDiffBlockEdges edges
+        int cs = 1;
+        while (cs < kSmallDiffCluster && (cs * kSmallDiffThreads < positions || cs * kSmallDiffBlockEdges < g.m)) cs *= 2;
+        if (cs > 8) GP_CUDA(cudaFuncSetAttribute(small, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(cs);
         cfg.blockDim = dim3(kSmallDiffThreads);
@@ -856,20 +859,26 @@ void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask*
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cudaEvent_t ev0 = nullptr;
-        if (d.prof) { ev0 = d.event(); GP_CUDA(cudaEventRecord(ev0, d.stream)); }
-        const O* off = g.off.get();
-        GP_CUDA(cudaLaunchKernelEx(&cfg, small, ntasks, tasks, task_of_pos, positions, order, labels, off,
-                                   g.nbr.get(), g.ewp(), seed, steps, x_out, key));
-        ++d.launches;
-        if (d.prof) {
-            cudaEvent_t ev1 = d.event();
-            GP_CUDA(cudaEventRecord(ev1, d.stream));
-            auto& e = d.prof_table["diffusion_small_kernel"];
-            e.pending.push_back({ev0, ev1});
-            ++e.launches;
+        // a cluster that cannot be placed (too few free SMs in a GPC) leaves
+        // the graph to the cooperative kernel, which computes the same values
+        int placeable = 0;
+        GP_CUDA(cudaOccupancyMaxActiveClusters(&placeable, small, &cfg));
+        if (placeable > 0) {
+            cudaEvent_t ev0 = nullptr;
+            if (d.prof) { ev0 = d.event(); GP_CUDA(cudaEventRecord(ev0, d.stream)); }
+            const O* off = g.off.get();
+            GP_CUDA(cudaLaunchKernelEx(&cfg, small, ntasks, tasks, task_of_pos, positions, order, labels, off,
+                                       g.nbr.get(), g.ewp(), seed, steps, x_out, key));
+            ++d.launches;
+            if (d.prof) {
+                cudaEvent_t ev1 = d.event();
+                GP_CUDA(cudaEventRecord(ev1, d.stream));
+                auto& e = d.prof_table["diffusion_small_kernel"];
+                e.pending.push_back({ev0, ev1});
+                ++e.launches;
+            }
+            return;
         }
-        return;
     }
     auto kernel = diffusion_kernel<O, W>;
     int per_sm = 0;

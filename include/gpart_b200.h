@@ -210,9 +210,9 @@ gp_status gp_ctx_set_sync_mode(gp_ctx* ctx, int blocking);
  * device's block slots, so that kernels of other contexts run beside them;
  * results do not depend on it.  The server sets it to its slot count. */
 gp_status gp_ctx_set_device_share(gp_ctx* ctx, int share);
-/* Small coarsest graphs (at most 4096 vertices, 65,536 edges and rows of at
- * most 4096 edges) run the spectral diffusion in one thread block instead of
- * a cooperative grid; both compute the same values.  enable = 0 keeps the
+/* Small coarsest graphs (at most 4096 vertices, 2,097,152 edges and rows of
+ * at most 4096 edges) run the spectral diffusion in one thread-block cluster
+ * instead of a cooperative grid; both compute the same values.  enable = 0 keeps the
  * grid kernel for every graph (default 1). */
 gp_status gp_ctx_set_small_diffusion(gp_ctx* ctx, int enable);
 

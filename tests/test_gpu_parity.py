@@ -208,6 +208,36 @@ def test_small_diffusion_cluster_sizes(ctx, nx, ny):
             assert np.array_equal(ctx.initial_partition(g, k, 1.03, 5), grid.initial_partition(g, k, 1.03, 5))
 
 
+def dense_random_csr(n, half_degree, seed):
+    rng = np.random.default_rng(seed)
+    src = np.repeat(np.arange(n, dtype=np.int64), half_degree)
+    dst = rng.integers(0, n, size=src.size)
+    keep = src != dst
+    a = np.concatenate([src[keep], dst[keep]])
+    b = np.concatenate([dst[keep], src[keep]])
+    codes = np.unique(a * n + b)
+    rows, cols = codes // n, codes % n
+    off = np.zeros(n + 1, np.int64)
+    np.add.at(off, rows + 1, 1)
+    return np.cumsum(off), cols.astype(np.int64)
+
+
+@pytest.mark.parametrize("n,half_degree", [(2048, 150), (4000, 250)])
+def test_small_diffusion_dense_clusters(ctx, n, half_degree):
+    """Dense small graphs (rows walked by warps, clusters of 8 and 16
+    blocks) give the cooperative kernel's values too."""
+    off, nbr = dense_random_csr(n, half_degree, 17)
+    g = hb.HostGraph(off, nbr)
+    labels = np.where(np.arange(n) % 4 == 0, 2, 0).astype(np.int32)
+    with hb.Context(0) as grid:
+        grid.set_small_diffusion(False)
+        for group, seed in ((0, 1), (2, 4)):
+            a = ctx.diffusion(g, labels, group, seed, 64)
+            b = grid.diffusion(g, labels, group, seed, 64)
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        assert np.array_equal(ctx.initial_partition(g, 8, 1.03, 2), grid.initial_partition(g, 8, 1.03, 2))
+
+
 def test_small_diffusion_on_coarse_level(ctx):
     off, idx, g = file_graph("rmat14")
     coff, cnbr, cew, cvw, _ = ctx.coarsen(g, parts=32)[-1]
