@@ -675,14 +675,4 @@ __global__ void max_weight_kernel(i64 m, const W* ew, u64* out) {
     if ((threadIdx.x & 31) == 0 && mx) atomic_max_u64(out, mx);
 }
 
-template <typename W>
-__global__ void sum_weight_kernel(i64 m, const W* ew, u64* out) {
-    __shared__ u64 sh[kWarps + 1];
-    u64 s = 0;
-    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<i64>(gridDim.x) * blockDim.x)
-        s += static_cast<u64>(ew[i]);
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0 && s) atomic_add_u64(out, s);
-}
-
 }  // namespace gp
