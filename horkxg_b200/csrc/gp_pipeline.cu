@@ -1714,8 +1714,11 @@ void initial_partition_static(const gp_graph* gi, int parts, double ratio, u32 s
     if (n64 > kStaticMaxVertices)
         fail(GP_EINVAL, "graph has " + std::to_string(n64) + " vertices; the allocation-free initial partition "
                         "supports at most " + std::to_string(kStaticMaxVertices));
-    if (n64 <= 0 || parts < 2 || parts > n64 || parts > 32 || !std::isfinite(ratio) || ratio < 1.0)
+    if (n64 <= 0 || gi->m < 0 || parts < 2 || parts > n64 || parts > 32 || !std::isfinite(ratio) || ratio < 1.0)
         fail(GP_EINVAL, "invalid GPU initial partition input");
+    if constexpr (std::is_same_v<T, Std>) {
+        if (gi->m > std::numeric_limits<i32>::max()) fail(GP_EINVAL, "graph exceeds standard CSR limits");
+    }
     const i32 n = static_cast<i32>(n64);
     const StaticScratch sc = carve_static(static_scratch_address());
 
@@ -1744,6 +1747,19 @@ void initial_partition_static(const gp_graph* gi, int parts, double ratio, u32 s
     g.unit_vw = gi->vertex_weights == nullptr;
     if (!g.unit_ew) g.ew.borrow(static_cast<W*>(const_cast<void*>(gi->edge_weights)), static_cast<size_t>(gi->m));
     if (!g.unit_vw) g.vw.borrow(static_cast<W*>(const_cast<void*>(gi->vertex_weights)), static_cast<size_t>(n));
+
+    // The caller's CSR is read in place, so check its shape before any kernel
+    // follows an offset or a neighbour id: offsets monotone from 0 to m, ids
+    // in [0, n).  The checks record a flag and never read out of bounds.
+    launch(d, "check_offsets_kernel", check_offsets_kernel<O>, blocks_for(n64 + 1, kThreads), kThreads, 0, n64,
+           g.off.get(), g.m, sc.err);
+    if (g.m)
+        launch(d, "check_neighbors_kernel", check_neighbors_kernel, stride_grid(d, g.m), kThreads, 0, g.m, g.nbr.get(),
+               n64, sc.err);
+    u32 shape_err = 0;
+    read(&shape_err, sc.err, sizeof(shape_err));
+    if (shape_err)
+        fail(GP_EINVAL, "weighted CSR shape is invalid (offsets not monotone from 0 to m or neighbor out of range)");
 
     launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, n), kThreads, 0, n, g.vwp(), sc.stats);
     launch(d, "sat_sum_kernel", sat_sum_kernel<W>, stride_grid(d, g.m), kThreads, 0, g.m, g.ewp(), sc.stats + 2);

