@@ -229,3 +229,20 @@ def cycle_hub(n: int = 4096, spokes: int = 512) -> tuple[Path, Path]:
         indices.extend(r)
         offsets.append(len(indices))
     return write_csr(f"cycle_hub_{n}_{spokes}", offsets, indices)
+
+
+def main(argv=None) -> int:
+    """``python -m horkxg_b200.graphs NAME...`` generates (or finds in the
+    cache) the named workloads and prints one JSON object mapping each name to
+    its [indptr, indices] paths, so that a caller can get the input files
+    without loading the generator library into its own process."""
+    import json
+    import sys
+    names = sys.argv[1:] if argv is None else argv
+    out = {name: [str(p) for p in by_name(name)] for name in names}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -418,7 +418,15 @@ void diffuse(const Graph& g, const std::vector<i32>& labels, const std::vector<i
     }
 }
 
-std::vector<i32> initial_partition(const Graph& g, int parts, double ratio, u32 seed) {
+// With `trace` (depths x n FP32 values, as gp_initial_partition_trace
+// returns them) each task is ordered by the traced value of its depth instead
+// of the FP64 diffusion, so that the split rules are checked on exactly the
+// vector the device sorted; the FP64 diffusion is still computed for every
+// task and the largest relative L2 distance between the two is reported in
+// *max_rel_l2.
+std::vector<i32> initial_partition(const Graph& g, int parts, double ratio, u32 seed,
+                                   const float* trace = nullptr, int trace_depths = 0,
+                                   double* max_rel_l2 = nullptr) {
     const i64 n = g.n;
     if (n <= 0 || n > std::numeric_limits<int>::max() - 255 || parts < 2 || parts > n || parts > 32 ||
         !std::isfinite(ratio) || ratio < 1.0)
@@ -434,8 +442,9 @@ std::vector<i32> initial_partition(const Graph& g, int parts, double ratio, u32 
     std::vector<i32> labels(static_cast<size_t>(n), 0), order(static_cast<size_t>(n));
     std::iota(order.begin(), order.end(), 0);
     std::vector<double> x(static_cast<size_t>(n), 0.0);
-    struct Task { int begin, count, first_part, parts; u64 weight; };
-    std::vector<Task> tasks{{0, static_cast<int>(n), 0, parts, total}};
+    struct Task { int begin, count, first_part, parts; u64 weight; int depth; };
+    std::vector<Task> tasks{{0, static_cast<int>(n), 0, parts, total, 0}};
+    if (max_rel_l2) *max_rel_l2 = 0.0;
     while (!tasks.empty()) {
         const Task t = tasks.back();
         tasks.pop_back();
@@ -445,6 +454,19 @@ std::vector<i32> initial_partition(const Graph& g, int parts, double ratio, u32 
         }
         std::vector<i32> ids(order.begin() + t.begin, order.begin() + t.begin + t.count);
         diffuse(g, labels, ids, t.first_part, seed ^ static_cast<u32>(t.first_part), 64, x);
+        if (trace) {
+            if (t.depth >= trace_depths) throw std::runtime_error("trace has fewer depths than the task tree");
+            const float* row = trace + static_cast<size_t>(t.depth) * static_cast<size_t>(n);
+            double diff = 0, norm = 0;
+            for (i32 v : ids) {
+                const float f = row[v];
+                if (f != f) throw std::runtime_error("trace has no value for a vertex of an open task");
+                diff += (static_cast<double>(f) - x[v]) * (static_cast<double>(f) - x[v]);
+                norm += x[v] * x[v];
+                x[v] = static_cast<double>(f);
+            }
+            if (max_rel_l2 && norm > 1e-24) *max_rel_l2 = std::max(*max_rel_l2, std::sqrt(diff / norm));
+        }
         std::sort(ids.begin(), ids.end(), [&](i32 a, i32 b) { return x[a] < x[b] || (x[a] == x[b] && a < b); });
         std::copy(ids.begin(), ids.end(), order.begin() + t.begin);
         std::vector<u64> prefix(static_cast<size_t>(t.count));
@@ -465,8 +487,9 @@ std::vector<i32> initial_partition(const Graph& g, int parts, double ratio, u32 
             throw std::runtime_error("GPU spectral split cannot satisfy capacity");
         for (int i = 0; i < t.count; ++i)
             labels[ids[i]] = i < boundary ? t.first_part : t.first_part + left_parts;
-        tasks.push_back({t.begin + boundary, t.count - boundary, t.first_part + left_parts, right_parts, t.weight - left_weight});
-        tasks.push_back({t.begin, boundary, t.first_part, left_parts, left_weight});
+        tasks.push_back({t.begin + boundary, t.count - boundary, t.first_part + left_parts, right_parts,
+                         t.weight - left_weight, t.depth + 1});
+        tasks.push_back({t.begin, boundary, t.first_part, left_parts, left_weight, t.depth + 1});
     }
     std::vector<u64> loads(static_cast<size_t>(parts), 0);
     for (i64 v = 0; v < n; ++v) loads[labels[v]] += g.vw[v];
@@ -927,6 +950,17 @@ int or_initial_partition(int64_t n, const int64_t* offsets, const int32_t* neigh
     });
 }
 
+int or_initial_partition_replay(int64_t n, const int64_t* offsets, const int32_t* neighbors,
+                                const uint64_t* edge_weights, const uint64_t* vertex_weights,
+                                int parts, double ratio, uint32_t seed, const float* trace,
+                                int trace_depths, int32_t* labels, double* max_rel_l2) {
+    return guarded([&] {
+        const Graph g = make_graph(n, offsets, neighbors, edge_weights, vertex_weights);
+        const auto l = initial_partition(g, parts, ratio, seed, trace, trace_depths, max_rel_l2);
+        std::copy(l.begin(), l.end(), labels);
+    });
+}
+
 int or_refine(int64_t n, const int64_t* offsets, const int32_t* neighbors,
               const uint64_t* edge_weights, const uint64_t* vertex_weights,
               int32_t* labels, int parts, double ratio, int max_rounds,
@@ -940,9 +974,10 @@ int or_refine(int64_t n, const int64_t* offsets, const int32_t* neighbors,
     });
 }
 
-int or_partition(int64_t n, const int64_t* offsets, const int32_t* neighbors,
-                 const uint64_t* edge_weights, const uint64_t* vertex_weights,
-                 int parts, double ratio, uint32_t seed, int32_t* labels, uint64_t* cut) {
+int or_partition_from(int64_t n, const int64_t* offsets, const int32_t* neighbors,
+                      const uint64_t* edge_weights, const uint64_t* vertex_weights,
+                      int parts, double ratio, uint32_t seed, const int32_t* coarsest_labels,
+                      int64_t coarsest_n, int32_t* labels, uint64_t* cut) {
     return guarded([&] {
         auto g = make_graph(n, offsets, neighbors, edge_weights, vertex_weights);
         u64 total = 0;
@@ -950,7 +985,13 @@ int or_partition(int64_t n, const int64_t* offsets, const int32_t* neighbors,
         partition_capacity(total, parts, ratio);
         const int beta = std::max(64, (512 + parts - 1) / parts);
         Hierarchy h = coarsen(std::move(g), parts, seed, beta, true, 24, 0.90);
-        std::vector<i32> cur = initial_partition(h.levels.back(), parts, ratio, seed);
+        std::vector<i32> cur;
+        if (coarsest_labels) {
+            if (coarsest_n != h.levels.back().n) throw InvalidArg("coarsest labels do not match the coarsest level");
+            cur.assign(coarsest_labels, coarsest_labels + coarsest_n);
+        } else {
+            cur = initial_partition(h.levels.back(), parts, ratio, seed);
+        }
         refine(h.levels.back(), cur, parts, ratio, 32);
         i64 last_refined = h.levels.back().n;
         for (size_t lv = h.levels.size() - 1; lv > 0; --lv) {
@@ -967,6 +1008,13 @@ int or_partition(int64_t n, const int64_t* offsets, const int32_t* neighbors,
         std::copy(cur.begin(), cur.end(), labels);
         *cut = undirected_cut(h.levels.front(), cur);
     });
+}
+
+int or_partition(int64_t n, const int64_t* offsets, const int32_t* neighbors,
+                 const uint64_t* edge_weights, const uint64_t* vertex_weights,
+                 int parts, double ratio, uint32_t seed, int32_t* labels, uint64_t* cut) {
+    return or_partition_from(n, offsets, neighbors, edge_weights, vertex_weights, parts, ratio, seed, nullptr, 0,
+                             labels, cut);
 }
 
 }  // extern "C"

@@ -76,6 +76,14 @@ int or_initial_partition(int64_t n, const int64_t* offsets, const int32_t* neigh
                          const uint64_t* edge_weights, const uint64_t* vertex_weights,
                          int parts, double ratio, uint32_t seed, int32_t* labels);
 
+/* The same recursion, each task ordered by a traced FP32 vector (depths x n,
+ * NaN outside open tasks) instead of the FP64 diffusion; *max_rel_l2 gets the
+ * largest relative L2 distance between a task's traced and FP64 vectors. */
+int or_initial_partition_replay(int64_t n, const int64_t* offsets, const int32_t* neighbors,
+                                const uint64_t* edge_weights, const uint64_t* vertex_weights,
+                                int parts, double ratio, uint32_t seed, const float* trace,
+                                int trace_depths, int32_t* labels, double* max_rel_l2);
+
 typedef struct {
     int rounds;
     uint64_t proposals, accepted, initial_cut, final_cut, final_max_part_weight;
@@ -97,6 +105,13 @@ int or_partition(int64_t n, const int64_t* offsets, const int32_t* neighbors,
                  const uint64_t* edge_weights, const uint64_t* vertex_weights,
                  int parts, double ratio, uint32_t seed, int32_t* labels,
                  uint64_t* cut);
+
+/* or_partition starting from given labels of the coarsest level (coarsest_n
+ * entries) instead of the FP64 initial partition (NULL = compute it). */
+int or_partition_from(int64_t n, const int64_t* offsets, const int32_t* neighbors,
+                      const uint64_t* edge_weights, const uint64_t* vertex_weights,
+                      int parts, double ratio, uint32_t seed, const int32_t* coarsest_labels,
+                      int64_t coarsest_n, int32_t* labels, uint64_t* cut);
 
 #ifdef __cplusplus
 }

@@ -60,6 +60,11 @@ def lib():
                                 ctypes.c_int, ctypes.POINTER(RefineStats)]
         L.or_partition.argtypes = [ctypes.c_int64, I64P, I32P, U64P, U64P, ctypes.c_int, ctypes.c_double,
                                    ctypes.c_uint32, I32P, U64P]
+        L.or_partition_from.argtypes = [ctypes.c_int64, I64P, I32P, U64P, U64P, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_uint32, I32P, ctypes.c_int64, I32P, U64P]
+        L.or_initial_partition_replay.argtypes = [ctypes.c_int64, I64P, I32P, U64P, U64P, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_uint32,
+                                                  ctypes.POINTER(ctypes.c_float), ctypes.c_int, I32P, F64P]
         _LIB = L
     return _LIB
 
@@ -163,6 +168,19 @@ def initial_partition(g: Graph, parts: int, ratio: float = 1.03, seed: int = 0):
     return labels
 
 
+def initial_partition_replay(g: Graph, parts: int, trace, ratio: float = 1.03, seed: int = 0):
+    """The initial partition's recursion with each task ordered by the traced
+    FP32 vector of its depth (rows of `trace`); returns (labels, largest
+    relative L2 distance of a traced vector from the FP64 diffusion)."""
+    trace = np.ascontiguousarray(trace, dtype=np.float32)
+    labels = np.zeros(g.n, np.int32)
+    err = ctypes.c_double()
+    _check(lib().or_initial_partition_replay(*g.args(), parts, ratio, seed,
+                                             trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                             int(trace.shape[0]), _p(labels, I32P), ctypes.byref(err)))
+    return labels, err.value
+
+
 def refine(g: Graph, labels, parts: int, ratio: float = 1.03, max_rounds: int = 32):
     labels = np.array(labels, dtype=np.int32, copy=True)
     st = RefineStats()
@@ -174,6 +192,18 @@ def partition(g: Graph, parts: int, ratio: float = 1.03, seed: int = 0):
     labels = np.zeros(g.n, np.int32)
     cut = ctypes.c_uint64()
     _check(lib().or_partition(*g.args(), parts, ratio, seed, _p(labels, I32P), ctypes.byref(cut)))
+    return labels, cut.value
+
+
+def partition_from(g: Graph, parts: int, coarsest_labels, ratio: float = 1.03, seed: int = 0):
+    """The oracle's pipeline (coarsen, refine the coarsest level, project and
+    refine by the schedule of src/refine.cu:423-646) from given labels of the
+    coarsest level."""
+    cl = np.ascontiguousarray(coarsest_labels, dtype=np.int32)
+    labels = np.zeros(g.n, np.int32)
+    cut = ctypes.c_uint64()
+    _check(lib().or_partition_from(*g.args(), parts, ratio, seed, _p(cl, I32P), len(cl), _p(labels, I32P),
+                                   ctypes.byref(cut)))
     return labels, cut.value
 
 

@@ -14,7 +14,12 @@ records:
 
 Needs a GPU.  Usage: ``python tests/golden/make_golden.py --out DIR``; the JSON
 written to DIR/reference_goldens.json is committed as
-``tests/golden/reference_goldens.json``.
+``tests/golden/reference_goldens.json``.  With ``--scale`` it records the
+same digests for the configured sizes instead (RMAT-20 at seeds 0-2, RMAT-22
+k=32, the 320^3 grid at big width) plus the RMAT-20 cuts at seeds 0-4, into
+DIR/reference_goldens_scale.json (committed as
+``tests/golden/reference_goldens_scale.json``); the hierarchy files, several
+GB, are deleted after hashing.
 """
 from __future__ import annotations
 
@@ -54,6 +59,18 @@ HIERARCHY_CASES = [
     ("cycle_hub_4096", 4, 0, 256, 0, "big"),
 ]
 
+SCALE_HIERARCHY_CASES = [
+    ("rmat20", 32, 0, -1, 1, "standard"),
+    ("rmat20", 32, 1, -1, 1, "standard"),
+    ("rmat20", 32, 2, -1, 1, "standard"),
+    ("rmat22", 32, 0, -1, 1, "standard"),
+    ("grid3d_320", 8, 0, -1, 1, "big"),
+]
+
+SCALE_PARTITION_CASES = [
+    ("rmat20", 32, "standard"),
+]
+
 PARTITION_CASES = [
     ("grid2d_256", 4, "standard"),
     ("grid3d_24", 8, "standard"),
@@ -64,14 +81,16 @@ PARTITION_CASES = [
 
 
 def level_digests(path: Path) -> list[dict]:
-    data = np.fromfile(path, dtype=np.int32)
+    data = np.memmap(path, dtype=np.int32, mode="r")
     pos = 1
     out = []
     for level in range(int(data[0])):
         n, m = int(data[pos]), int(data[pos + 1])
         size = 2 + (n + 1) + m + m + n + (n_prev if level > 0 else 0)
-        chunk = data[pos:pos + size]
-        out.append({"n": n, "m": m, "sha256": hashlib.sha256(chunk.tobytes()).hexdigest()})
+        h = hashlib.sha256()
+        for at in range(pos, pos + size, 1 << 26):        # in pieces: level files reach GBs
+            h.update(np.ascontiguousarray(data[at:min(pos + size, at + (1 << 26))]).tobytes())
+        out.append({"n": n, "m": m, "sha256": h.hexdigest()})
         pos += size
         n_prev = n
     if pos != len(data):
@@ -79,23 +98,34 @@ def level_digests(path: Path) -> list[dict]:
     return out
 
 
+def file_sha256(path: Path) -> str:
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for block in iter(lambda: f.read(1 << 26), b""):
+            h.update(block)
+    return h.hexdigest()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", type=Path, required=True)
     ap.add_argument("--keep", action="store_true", help="keep hierarchy files under --out")
+    ap.add_argument("--scale", action="store_true", help="the configured sizes instead of the small fixtures")
     args = ap.parse_args()
     args.out.mkdir(parents=True, exist_ok=True)
+    hierarchy_cases = SCALE_HIERARCHY_CASES if args.scale else HIERARCHY_CASES
+    partition_cases = SCALE_PARTITION_CASES if args.scale else PARTITION_CASES
     result = {"fixtures": {}, "hierarchies": [], "partitions": []}
-    names = sorted({c[0] for c in HIERARCHY_CASES} | {c[0] for c in PARTITION_CASES})
+    names = sorted({c[0] for c in hierarchy_cases} | {c[0] for c in partition_cases})
     for name in names:
         indptr, indices = graphs.by_name(name)
         result["fixtures"][name] = {
             "n": int(indptr.stat().st_size // 8 - 1),
             "m": int(indices.stat().st_size // 8),
-            "sha256_indptr": hashlib.sha256(indptr.read_bytes()).hexdigest(),
-            "sha256_indices": hashlib.sha256(indices.read_bytes()).hexdigest(),
+            "sha256_indptr": file_sha256(indptr),
+            "sha256_indices": file_sha256(indices),
         }
-    for name, parts, seed, beta, pack, variant in HIERARCHY_CASES:
+    for name, parts, seed, beta, pack, variant in hierarchy_cases:
         indptr, indices = graphs.by_name(name)
         out = args.out / f"hier_{name}_k{parts}_s{seed}_b{beta}_p{pack}_{variant}.bin"
         cmd = [str(REF / f"ref_hierarchy_{variant}"), str(indptr), str(indices), str(parts), str(seed),
@@ -109,7 +139,7 @@ def main() -> None:
         if not args.keep or out.stat().st_size > (3 << 20):
             out.unlink()
         print("hierarchy", name, parts, seed, variant, len(result["hierarchies"][-1]["levels"]), flush=True)
-    for name, parts, variant in PARTITION_CASES:
+    for name, parts, variant in partition_cases:
         indptr, indices = graphs.by_name(name)
         for seed in range(5):
             part = Path("/tmp") / f"gp_golden_{name}_{parts}_{seed}.part"
@@ -127,7 +157,8 @@ def main() -> None:
                 "cut": cut, "max_load": int(loads.max()), "algorithm_total_seconds": algo,
                 "process_seconds": wall})
             print("partition", name, parts, seed, cut, algo, flush=True)
-    (args.out / "reference_goldens.json").write_text(json.dumps(result, indent=1) + "\n")
+    target = "reference_goldens_scale.json" if args.scale else "reference_goldens.json"
+    (args.out / target).write_text(json.dumps(result, indent=1) + "\n")
 
 
 if __name__ == "__main__":

@@ -218,3 +218,23 @@ def test_oracle_partition_quality_near_reference():
     ref = sorted(p["cut"] for p in GOLD["partitions"] if p["fixture"] == "grid2d_256")
     assert cut <= 1.10 * ref[len(ref) // 2]
     assert np.bincount(lab).max() <= O.partition_capacity(len(off) - 1, 4, 1.03)
+
+
+def test_oracle_initial_partition_replay_on_its_own_vector():
+    # one bisection: a trace holding the FP64 root vector in FP32 gives the
+    # FP64 recursion's split (the grid's vector has no near-ties at the split)
+    off, idx = graphs.load(*graphs.by_name("grid2d_64"))
+    g = O.Graph(off, np.asarray(idx))
+    for seed in (0, 3):
+        x = O.diffusion(g, np.zeros(g.n, np.int32), 0, seed, 64).astype(np.float32)
+        labels, err = O.initial_partition_replay(g, 2, x[None, :], 1.03, seed)
+        assert np.array_equal(labels, O.initial_partition(g, 2, 1.03, seed))
+        assert err < 1e-6
+
+
+def test_oracle_partition_from_its_own_initial_partition():
+    off, idx = graphs.load(*graphs.by_name("rmat12"))
+    g = O.Graph(off, np.asarray(idx))
+    levels, _ = O.coarsen(g, 8)
+    init = O.initial_partition(levels[-1], 8)
+    assert np.array_equal(O.partition_from(g, 8, init)[0], O.partition(g, 8)[0])
