@@ -63,6 +63,25 @@ class RequestInfo(ctypes.Structure):
                 ("footprint_bytes", ctypes.c_uint64), ("message", ctypes.c_char * 192)]
 
 
+class PartStats(ctypes.Structure):
+    _fields_ = [("vertices", ctypes.c_uint64), ("internal_edges", ctypes.c_uint64),
+                ("outgoing_cut_edges", ctypes.c_uint64), ("incoming_cut_edges", ctypes.c_uint64),
+                ("weighted_internal", ctypes.c_uint64), ("weighted_outgoing", ctypes.c_uint64),
+                ("weighted_incoming", ctypes.c_uint64)]
+
+
+class Analysis(ctypes.Structure):
+    _fields_ = [("parts", ctypes.c_int32), ("reserved", ctypes.c_int32), ("directed_edge_cut", ctypes.c_uint64),
+                ("weighted_directed_edge_cut", ctypes.c_uint64), ("max_local_cut", ctypes.c_uint64),
+                ("weighted_max_local_cut", ctypes.c_uint64), ("avg_local_cut", ctypes.c_double),
+                ("weighted_avg_local_cut", ctypes.c_double), ("vertex_avg", ctypes.c_double),
+                ("min_vertices", ctypes.c_uint64), ("max_vertices", ctypes.c_uint64),
+                ("vertex_imbalance", ctypes.c_double), ("vertex_max_deviation", ctypes.c_double),
+                ("edge_set_avg", ctypes.c_double), ("min_edge_set", ctypes.c_uint64),
+                ("max_edge_set", ctypes.c_uint64), ("edge_set_imbalance", ctypes.c_double),
+                ("edge_set_max_deviation", ctypes.c_double)]
+
+
 class RefineStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_int32), ("proposals", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
                 ("initial_cut", ctypes.c_uint64), ("final_cut", ctypes.c_uint64),
@@ -74,7 +93,7 @@ EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_erro
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
            "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
-           "gp_initial_partition_static", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
+           "gp_initial_partition_static", "gp_initial_partition_trace", "gp_analyze", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
            "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
            "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
 
@@ -104,9 +123,11 @@ def lib() -> ctypes.CDLL:
         L.gp_hierarchy_write.argtypes = [vp, ctypes.c_char_p]
         L.gp_hierarchy_free.argtypes = [vp]
         L.gp_initial_partition.argtypes = [vp, P(GraphDesc), i32, dbl, u32, vp]
+        L.gp_initial_partition_trace.argtypes = [vp, P(GraphDesc), i32, dbl, u32, vp, vp, i32, P(ctypes.c_int32)]
         L.gp_diffusion.argtypes = [vp, P(GraphDesc), vp, i32, u32, i32, vp]
         L.gp_refine.argtypes = [vp, P(GraphDesc), vp, i32, dbl, i32, i32, P(RefineStats)]
         L.gp_cut.argtypes = [vp, P(GraphDesc), vp, i32, P(ctypes.c_uint64), vp]
+        L.gp_analyze.argtypes = [vp, P(GraphDesc), vp, i32, P(PartStats), P(Analysis)]
         L.gp_launch_count.argtypes = [vp]
         L.gp_launch_count.restype = ctypes.c_uint64
         L.gp_sync_count.argtypes = [vp]
@@ -159,6 +180,20 @@ def capacity(total: int, parts: int, ratio: float) -> int:
     if rc:
         raise PartitionError(rc, "invalid partition capacity")
     return out.value
+
+
+def plan_depths(parts: int) -> list[list[tuple[int, int]]]:
+    """The bisection task tree for `parts`, level by level: each task is
+    (first_part, parts); a task of one part is a leaf and not listed."""
+    levels, cur = [], [(0, parts)]
+    while cur:
+        levels.append(cur)
+        nxt = []
+        for first, p in cur:
+            lp, rp = p // 2, p - p // 2
+            nxt += [t for t in ((first, lp), (first + lp, rp)) if t[1] >= 2]
+        cur = nxt
+    return levels
 
 
 class HostGraph:
@@ -466,11 +501,38 @@ class Context:
         finally:
             lib().gp_hierarchy_free(h)
 
+    def coarsen_to_file(self, g: HostGraph, path, options: Options | None = None, **kw) -> int:
+        """Coarsens and writes the hierarchy in the reference's file layout
+        (include/hierarchy.hpp:42-126); returns the number of levels."""
+        o = options or default_options(**kw)
+        h = ctypes.c_void_p()
+        d = g.desc()
+        self._check(lib().gp_coarsen(self._h, ctypes.byref(d), ctypes.byref(o), ctypes.byref(h)))
+        try:
+            if lib().gp_hierarchy_write(h, str(path).encode()) != GP_OK:
+                raise PartitionError(GP_ERUNTIME, f"cannot write {path}")
+            return lib().gp_hierarchy_levels(h)
+        finally:
+            lib().gp_hierarchy_free(h)
+
     def initial_partition(self, g: HostGraph, parts: int, ratio: float = 1.03, seed: int = 0):
         labels = np.zeros(g.n, np.int32)
         d = g.desc()
         self._check(lib().gp_initial_partition(self._h, ctypes.byref(d), parts, ratio, seed, labels.ctypes.data))
         return labels
+
+    def initial_partition_trace(self, g: HostGraph, parts: int, ratio: float = 1.03, seed: int = 0):
+        """Labels plus the FP32 diffusion value of every vertex at every
+        recursion depth (rows of a depths x n array, NaN outside open tasks)."""
+        labels = np.zeros(g.n, np.int32)
+        depths = ctypes.c_int32()
+        d = g.desc()
+        rows = len(plan_depths(min(max(parts, 2), 32)))
+        trace = np.zeros((rows, g.n), np.float32)
+        self._check(lib().gp_initial_partition_trace(self._h, ctypes.byref(d), parts, ratio, seed,
+                                                     labels.ctypes.data, trace.ctypes.data, rows,
+                                                     ctypes.byref(depths)))
+        return labels, trace[:depths.value]
 
     def diffusion(self, g: HostGraph, labels, group: int, seed: int, steps: int = 64):
         labels = np.ascontiguousarray(labels, np.int32)
@@ -497,3 +559,14 @@ class Context:
         self._check(lib().gp_cut(self._h, ctypes.byref(d), labels.ctypes.data, parts, ctypes.byref(c),
                                  loads.ctypes.data))
         return c.value, loads
+
+    def analyze(self, g: HostGraph, labels, parts: int):
+        """The reference analyzer's report on the GPU: (per-part stats as a
+        dict of uint64 arrays, summary dict)."""
+        labels = np.ascontiguousarray(labels, np.int32)
+        st = (PartStats * parts)()
+        a = Analysis()
+        d = g.desc()
+        self._check(lib().gp_analyze(self._h, ctypes.byref(d), labels.ctypes.data, parts, st, ctypes.byref(a)))
+        per = {f: np.array([getattr(x, f) for x in st], np.uint64) for f, _ in PartStats._fields_}
+        return per, {f: getattr(a, f) for f, _ in Analysis._fields_ if f != "reserved"}

@@ -27,6 +27,7 @@
 #include "gp_initial.cuh"
 #include "gp_refine.cuh"
 #include "gp_hub.cuh"
+#include "gp_analyze.cuh"
 
 namespace gp {
 
@@ -766,6 +767,134 @@ struct Hierarchy {
     std::string stop_reason = "capacity_floor";
 };
 
+// ---------------------------------------------------------------------------
+// --verify: checks of every coarsening step on the device, with the rules and
+// messages of validate_coarsening_step (src/coarsen.cu:1835-1902).
+// ---------------------------------------------------------------------------
+template <typename O>
+__global__ void check_offsets_kernel(i64 n, const O* off, i64 m, u32* err);
+__global__ void check_neighbors_kernel(i64 m, const i32* nbr, i64 n, u32* err);
+template <typename O, typename W>
+__global__ void symmetry_kernel(i64 n, const O* off, const i32* nbr, const W* ew, u32* err);
+
+enum VerifyFlag : u32 {
+    kVerifyMapRange = 1u << 0,
+    kVerifyCluster = 1u << 1,
+    kVerifyCap = 1u << 2,
+    kVerifySelfLoop = 1u << 3,
+};
+
+template <typename W>
+__global__ void verify_map_kernel(i64 n, const i32* __restrict__ map, i64 coarse_n, const W* __restrict__ vw,
+                                  u64* recomputed, u32* coverage, u32* flags) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const i32 c = map[v];
+    if (c < 0 || c >= coarse_n) {
+        atomicOr(flags, kVerifyMapRange);
+        return;
+    }
+    atomic_add_u64(&recomputed[c], static_cast<u64>(weight_at(vw, v)));
+    atomicAdd(&coverage[c], 1u);
+}
+
+template <typename W>
+__global__ void verify_clusters_kernel(i64 coarse_n, const u64* __restrict__ recomputed,
+                                       const u32* __restrict__ coverage, const W* __restrict__ cvw, u64 cap,
+                                       u32* flags) {
+    const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= coarse_n) return;
+    const u64 w = static_cast<u64>(weight_at(cvw, c));
+    if (coverage[c] == 0 || recomputed[c] != w) atomicOr(flags, kVerifyCluster);
+    if (w > cap) atomicOr(flags, kVerifyCap);
+}
+
+template <typename O>
+__global__ void self_loop_kernel(i64 n, const O* __restrict__ off, const i32* __restrict__ nbr, u32* flags) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    for (i64 e = off[v]; e < static_cast<i64>(off[v + 1]); ++e)
+        if (nbr[e] == v) {
+            atomicOr(flags, kVerifySelfLoop);
+            return;
+        }
+}
+
+// Labels (c * 2654435761 + 17) mod 23 of coarse vertex c, through `map` for
+// the fine level (map == nullptr: the coarse level itself).
+__global__ void hashed_labels_kernel(i64 n, const i32* __restrict__ map, i32* labels) {
+    const i64 v = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const u64 c = map ? static_cast<u64>(map[v]) : static_cast<u64>(v);
+    labels[v] = static_cast<i32>((c * 2654435761ULL + 17ULL) % 23ULL);
+}
+
+template <typename T>
+u64 directed_cut(Device& d, const DGraph<T>& g, const i32* labels, u64* scratch);
+
+template <typename T>
+void verify_coarsening_step(Device& d, const DGraph<T>& fine, const DGraph<T>& coarse, const i32* map, u64 cap,
+                            int level, Log& log) {
+    using O = typename T::O;
+    using W = typename T::W;
+    if (coarse.n <= 0 || coarse.n > fine.n) fail(GP_ERUNTIME, "coarsening produced an invalid vertex count");
+    Buf<u64> recomputed(d, static_cast<size_t>(coarse.n)), sums(d, 4);
+    Buf<u32> coverage(d, static_cast<size_t>(coarse.n)), flags(d, 1);
+    recomputed.zero(d);
+    coverage.zero(d);
+    sums.zero(d);
+    flags.zero(d);
+    launch(d, "verify_map_kernel", verify_map_kernel<W>, blocks_for(fine.n, kThreads), kThreads, 0, fine.n, map,
+           coarse.n, fine.vwp(), recomputed.get(), coverage.get(), flags.get());
+    launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, fine.n), kThreads, 0, fine.n, fine.vwp(),
+           sums.get());
+    launch(d, "weight_stats_kernel", weight_stats_kernel<W>, stride_grid(d, coarse.n), kThreads, 0, coarse.n,
+           coarse.vwp(), sums.get() + 2);
+    GP_LAUNCH();
+    u32 f = 0;
+    fetch(d, &f, flags.get(), 1);
+    if (f & kVerifyMapRange) fail(GP_ERUNTIME, "coarsening map contains an out-of-range id");
+    u64 st[4];
+    fetch(d, st, sums.get(), 4);
+    if (st[0] != st[2]) fail(GP_ERUNTIME, "coarsening did not conserve vertex weight");
+    launch(d, "verify_clusters_kernel", verify_clusters_kernel<W>, blocks_for(coarse.n, kThreads), kThreads, 0,
+           coarse.n, recomputed.get(), coverage.get(), coarse.vwp(), cap, flags.get());
+    GP_LAUNCH();
+    fetch(d, &f, flags.get(), 1);
+    if (f & kVerifyCluster) fail(GP_ERUNTIME, "coarsening cluster weight mismatch");
+    if (f & kVerifyCap) fail(GP_ERUNTIME, "coarse point exceeds configured weight cap");
+    // strict CSR checks of the coarse level (validate_weighted_csr, src/graph.cpp:122-190)
+    launch(d, "check_offsets_kernel", check_offsets_kernel<O>, blocks_for(coarse.n + 1, kThreads), kThreads, 0,
+           coarse.n, coarse.off.get(), coarse.m, flags.get());
+    if (coarse.m)
+        launch(d, "check_neighbors_kernel", check_neighbors_kernel, stride_grid(d, coarse.m), kThreads, 0, coarse.m,
+               coarse.nbr.get(), coarse.n, flags.get());
+    GP_LAUNCH();
+    fetch(d, &f, flags.get(), 1);
+    if (f & kErrBadInput) fail(GP_ERUNTIME, "invalid weighted CSR shape");
+    launch(d, "self_loop_kernel", self_loop_kernel<O>, blocks_for(coarse.n, kThreads), kThreads, 0, coarse.n,
+           coarse.off.get(), coarse.nbr.get(), flags.get());
+    launch(d, "symmetry_kernel", symmetry_kernel<O, W>, blocks_for(coarse.n, kThreads), kThreads, 0, coarse.n,
+           coarse.off.get(), coarse.nbr.get(), coarse.ewp(), flags.get());
+    GP_LAUNCH();
+    fetch(d, &f, flags.get(), 1);
+    if (f & kVerifySelfLoop) fail(GP_ERUNTIME, "contracted graph contains a self loop");
+    if (f & kErrOddCut) fail(GP_ERUNTIME, "weighted CSR is not bidirectional");
+    // the cut of hashed coarse labels equals the cut of their projection
+    Buf<i32> fl(d, static_cast<size_t>(fine.n)), cl(d, static_cast<size_t>(coarse.n));
+    launch(d, "hashed_labels_kernel", hashed_labels_kernel, blocks_for(fine.n, kThreads), kThreads, 0, fine.n, map,
+           fl.get());
+    launch(d, "hashed_labels_kernel", hashed_labels_kernel, blocks_for(coarse.n, kThreads), kThreads, 0, coarse.n,
+           static_cast<const i32*>(nullptr), cl.get());
+    GP_LAUNCH();
+    const u64 fine_cut = directed_cut<T>(d, fine, fl.get(), sums.get());
+    const u64 coarse_cut = directed_cut<T>(d, coarse, cl.get(), sums.get() + 2);
+    if ((fine_cut & 1ULL) || (coarse_cut & 1ULL)) fail(GP_ERUNTIME, "weighted CSR cut is not symmetric");
+    if (fine_cut != coarse_cut) fail(GP_ERUNTIME, "cut is not conserved by coarse projection");
+    if (log.on)
+        log.out << "ml_layer_verify level=" << level << " map=ok weights=ok csr=ok projection_cut=ok\n";
+}
+
 template <typename T>
 void coarsen(Device& d, DGraph<T>&& input, const Opts& o, Hierarchy<T>& h, Log& log) {
     const int beta = o.beta > 0 ? o.beta : production_beta(o.parts);
@@ -796,6 +925,7 @@ void coarsen(Device& d, DGraph<T>&& input, const Opts& o, Hierarchy<T>& h, Log& 
         contract(d, current, agg.map.get(), agg.coarse_n, std::move(agg.cvw), coarse);
         if (log.on)
             log.out << "ml_gpu_contract_seconds level=" << level << " coarse_edges=" << coarse.m << '\n';
+        if (o.verify) verify_coarsening_step(d, current, coarse, agg.map.get(), agg.cap, level, log);
         h.levels.push_back(std::move(current));
         h.maps.push_back(std::move(agg.map));
         current = std::move(coarse);
@@ -907,9 +1037,12 @@ void launch_diffusion(Device& d, const DGraph<T>& g, int ntasks, const InitTask*
     }
 }
 
+// `trace` (optional, device, depths x n floats): for every recursion depth
+// the normalised diffusion value of each vertex of an open task at that
+// depth; the caller fills it with a marker beforehand.
 template <typename T>
 void initial_partition(Device& d, const DGraph<T>& g, int parts, double ratio, u32 seed, Buf<i32>& labels,
-                       u64* initial_cut, Log& log) {
+                       u64* initial_cut, Log& log, float* trace = nullptr) {
     using W = typename T::W;
     const i64 n64 = g.n;
     if (n64 <= 0 || n64 > std::numeric_limits<int>::max() - 255 || parts < 2 || parts > n64 || parts > 32 ||
@@ -953,8 +1086,9 @@ void initial_partition(Device& d, const DGraph<T>& g, int parts, double ratio, u
         GP_CUDA(cudaMemsetAsync(task_of_pos.get(), 0xff, n * sizeof(i32), d.stream));
         launch(d, "task_positions_kernel", task_positions_kernel, nt, kThreads, 0, nt, dtasks[dpt].get(), task_of_pos.get());
         GP_LAUNCH();
+        float* x_out = trace ? trace + dpt * static_cast<size_t>(n) : nullptr;
         launch_diffusion(d, g, nt, dtasks[dpt].get(), task_of_pos.get(), n, order.get(), labels.get(), seed, 64,
-                         deg.get(), xa.get(), xb.get(), contrib.get(), nullptr, key.get(), bar.get(), max_degree);
+                         deg.get(), xa.get(), xb.get(), contrib.get(), x_out, key.get(), bar.get(), max_degree);
         launch(d, "task_sort_kernel", task_sort_kernel, nt, kThreads, 0, nt, dtasks[dpt].get(), key.get(), key_alt.get(), order.get());
         InitTask* next = dpt + 1 < depths.size() ? dtasks[dpt + 1].get() : nullptr;
         launch(d, "task_split_kernel", task_split_kernel<W>, nt, kThreads, 0, nt, dtasks[dpt].get(), next, order.get(), g.vwp(), capacity,
@@ -1595,6 +1729,40 @@ void prepare_graph(Device& d, const gp_graph* gi, DGraph<T>& g, bool verify, i64
         if (e & kErrOddCut) fail(GP_ERUNTIME, "weighted CSR is not bidirectional");
         fail(GP_ERUNTIME, "weighted CSR shape is invalid (offsets not monotone or neighbor out of range)");
     }
+}
+
+// Per-part counts of the reference's analyzer (graph_untils/
+// analyze_partition.cpp:425-499) into `out` (kAnalyzeFields x parts, the
+// layout of gp_analyze.cuh).  `labels` is a device array of n entries.
+template <typename T>
+void analyze_parts(Device& d, const DGraph<T>& g, const i32* labels, int parts, std::vector<u64>& out) {
+    using O = typename T::O;
+    using W = typename T::W;
+    if (parts < 1 || parts > kAnalyzeMaxParts) fail(GP_EINVAL, "parts must be between 1 and 1024");
+    const size_t cells = static_cast<size_t>(kAnalyzeFields) * static_cast<size_t>(parts);
+    Buf<u64> acc(d, cells);
+    acc.zero(d);
+    const size_t smem = cells * sizeof(u64);
+    auto rows = analyze_rows_kernel<O, W>;
+    auto hubs_k = analyze_hub_kernel<W>;
+    GP_CUDA(cudaFuncSetAttribute(rows, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    GP_CUDA(cudaFuncSetAttribute(hubs_k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    if (g.n) {
+        // offsets, neighbour ids, their labels, weights, and each vertex's label
+        d.prof_bytes("analyze_rows_kernel", static_cast<double>(g.n + 1) * sizeof(O) +
+                                                static_cast<double>(g.m) * (8.0 + (g.ewp() ? sizeof(W) : 0)) +
+                                                static_cast<double>(g.n) * 4.0);
+        launch(d, "analyze_rows_kernel", rows, stride_grid(d, g.n * 32), kThreads, smem, g.n, g.off.get(), g.nbr.get(),
+               g.ewp(), labels, parts, acc.get(), d.err);
+        const auto& hubs = hub_index(d, g);
+        if (hubs.count)
+            launch(d, "analyze_hub_kernel", hubs_k, static_cast<int>(hubs.chunks), kThreads, smem, hubs.chunk.get(),
+                   g.nbr.get(), g.ewp(), labels, parts, acc.get(), d.err);
+        GP_LAUNCH();
+    }
+    d.check_errors();
+    out.resize(cells);
+    fetch(d, out.data(), acc.get(), cells);
 }
 
 template <typename T>
@@ -2256,6 +2424,35 @@ gp_status gp_initial_partition(gp_ctx* ctx, const gp_graph* graph, int parts, do
     });
 }
 
+gp_status gp_initial_partition_trace(gp_ctx* ctx, const gp_graph* graph, int parts, double ratio, uint32_t seed,
+                                     int32_t* labels, float* trace, int32_t trace_depths, int32_t* depths) {
+    if (!ctx || !depths) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        const int needed = static_cast<int>(gp::plan_tasks(std::max(2, std::min(parts, 32))).size());
+        *depths = needed;
+        if (trace && trace_depths < needed) gp::fail(GP_EINVAL, "trace holds fewer depths than the task tree");
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            const size_t cells = static_cast<size_t>(needed) * static_cast<size_t>(std::max<gp::i64>(g.n, 1));
+            gp::Buf<float> dev_trace;
+            if (trace) {
+                dev_trace = gp::Buf<float>(d, cells);
+                GP_CUDA(cudaMemsetAsync(dev_trace.get(), 0xff, cells * sizeof(float), d.stream));   // NaN marker
+            }
+            gp::Buf<gp::i32> lab;
+            gp::Log log;
+            gp::initial_partition<T>(d, g, parts, ratio, seed, lab, nullptr, log, trace ? dev_trace.get() : nullptr);
+            gp::to_host(d, labels, lab.get(), static_cast<size_t>(g.n));
+            if (trace) gp::to_host(d, trace, dev_trace.get(), static_cast<size_t>(needed) * static_cast<size_t>(g.n));
+            d.sync();
+        });
+    });
+}
+
 gp_status gp_diffusion(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int group, uint32_t seed, int steps,
                        float* x) {
     if (!ctx) return GP_EINVAL;
@@ -2390,6 +2587,75 @@ gp_status gp_profile_dump(gp_ctx* ctx, char* buffer, uint64_t capacity) {
         const size_t n = std::min<size_t>(s.size(), static_cast<size_t>(capacity) - 1);
         std::memcpy(buffer, s.data(), n);
         buffer[n] = 0;
+    });
+}
+
+gp_status gp_analyze(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts, gp_part_stats* per_part,
+                     gp_analysis* summary) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        if (!labels) gp::fail(GP_EINVAL, "null labels");
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            const gp::i32* dev_labels = labels;
+            gp::Buf<gp::i32> lab;
+            if (graph->memory != GP_MEMORY_DEVICE) {
+                lab = gp::Buf<gp::i32>(d, static_cast<size_t>(std::max<gp::i64>(g.n, 1)));
+                gp::to_device(d, lab.get(), labels, static_cast<size_t>(g.n));
+                dev_labels = lab.get();
+            }
+            std::vector<gp::u64> c;
+            try {
+                gp::analyze_parts<T>(d, g, dev_labels, parts, c);
+            } catch (const gp::Error& e) {
+                if (e.status == GP_EINVAL && std::string(e.what()) == "invalid graph input")
+                    gp::fail(GP_EINVAL, "partition id outside [0, parts)");
+                throw;
+            }
+            // analyze_partition.cpp:466-499
+            gp_analysis a{};
+            a.parts = parts;
+            const double np = static_cast<double>(parts);
+            a.min_vertices = a.min_edge_set = ~0ULL;
+            for (int q = 0; q < parts; ++q) {
+                gp_part_stats st{c[q], c[parts + q], c[2 * parts + q], c[3 * parts + q], c[4 * parts + q],
+                                 c[5 * parts + q], c[6 * parts + q]};
+                if (per_part) per_part[q] = st;
+                a.directed_edge_cut += st.outgoing_cut_edges;
+                a.weighted_directed_edge_cut += st.weighted_outgoing;
+                const gp::u64 edge_set = st.internal_edges + st.outgoing_cut_edges + st.incoming_cut_edges;
+                const gp::u64 local = st.outgoing_cut_edges + st.incoming_cut_edges;
+                const gp::u64 wlocal = st.weighted_outgoing + st.weighted_incoming;
+                a.avg_local_cut += static_cast<double>(local);
+                a.weighted_avg_local_cut += static_cast<double>(wlocal);
+                a.max_local_cut = std::max(a.max_local_cut, local);
+                a.weighted_max_local_cut = std::max(a.weighted_max_local_cut, wlocal);
+                a.min_vertices = std::min(a.min_vertices, st.vertices);
+                a.max_vertices = std::max(a.max_vertices, st.vertices);
+                a.min_edge_set = std::min(a.min_edge_set, edge_set);
+                a.max_edge_set = std::max(a.max_edge_set, edge_set);
+            }
+            a.avg_local_cut /= np;
+            a.weighted_avg_local_cut /= np;
+            auto deviation = [](double value, double average) {
+                if (average <= 0.0) return value == 0.0 ? 0.0 : std::numeric_limits<double>::infinity();
+                return std::abs(value - average) / average;
+            };
+            auto imbalance = [](double max_value, double average) { return average > 0.0 ? max_value / average : 0.0; };
+            a.vertex_avg = static_cast<double>(g.n) / np;
+            a.edge_set_avg = static_cast<double>(static_cast<gp::u64>(g.m) + a.directed_edge_cut) / np;
+            a.vertex_imbalance = imbalance(static_cast<double>(a.max_vertices), a.vertex_avg);
+            a.vertex_max_deviation = std::max(deviation(static_cast<double>(a.max_vertices), a.vertex_avg),
+                                              deviation(static_cast<double>(a.min_vertices), a.vertex_avg));
+            a.edge_set_imbalance = imbalance(static_cast<double>(a.max_edge_set), a.edge_set_avg);
+            a.edge_set_max_deviation = std::max(deviation(static_cast<double>(a.max_edge_set), a.edge_set_avg),
+                                                deviation(static_cast<double>(a.min_edge_set), a.edge_set_avg));
+            if (summary) *summary = a;
+        });
     });
 }
 

@@ -179,6 +179,17 @@ void gp_hierarchy_free(gp_hierarchy* h);
 gp_status gp_initial_partition(gp_ctx* ctx, const gp_graph* graph, int parts, double ratio,
                                uint32_t seed, int32_t* labels);
 
+/* gp_initial_partition with its diffusion vectors (same reference interface,
+ * include/initial_partition.hpp:9-12; the trace replaces no reference
+ * output).  For recursion depth d (0 = the root bisection) trace[d*n + v] is
+ * the normalised FP32 value that ordered vertex v in its task's split
+ * (src/initial_partition_gpu.cu:206-233), NaN when v was in no open task at
+ * that depth.  *depths receives the number of depths of the task tree for
+ * `parts`; trace (host, may be NULL to query) must hold trace_depths >= that
+ * many rows of n floats. */
+gp_status gp_initial_partition_trace(gp_ctx* ctx, const gp_graph* graph, int parts, double ratio, uint32_t seed,
+                                     int32_t* labels, float* trace, int32_t trace_depths, int32_t* depths);
+
 /* FP32 diffusion of one bisection task (src/initial_partition_gpu.cu:81-142):
  * vertices with labels[v] == group, seed ^ group, `steps` steps; x: n floats
  * (host), 0 outside the group. */
@@ -194,6 +205,44 @@ gp_status gp_refine(gp_ctx* ctx, const gp_graph* graph, int32_t* labels, int par
  * tools/verify_partition.py:22-65 and src/graph.cpp:192-212). */
 gp_status gp_cut(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts,
                  uint64_t* directed_cut, uint64_t* loads);
+
+/* Partition analysis on the GPU: the per-part report of the reference's CPU
+ * analyzer (replaces graph_untils/analyze_partition.cpp:425-499 over the
+ * directed CSR entries; edge weights are the graph's integer weights, unit
+ * when NULL, where the analyzer reads float values).  `labels` (n entries,
+ * host or device like the graph) must lie in [0, parts), 1 <= parts <= 1024,
+ * else GP_EINVAL.  per_part (parts entries) and summary may be NULL. */
+typedef struct gp_part_stats {
+    uint64_t vertices;             /* |V(pi)|: vertex count */
+    uint64_t internal_edges;       /* entries with both ends in the part */
+    uint64_t outgoing_cut_edges;   /* entries from the part to another */
+    uint64_t incoming_cut_edges;   /* entries from another part into it */
+    uint64_t weighted_internal;
+    uint64_t weighted_outgoing;
+    uint64_t weighted_incoming;
+} gp_part_stats;
+
+typedef struct gp_analysis {
+    int32_t parts;
+    int32_t reserved;
+    uint64_t directed_edge_cut;          /* global cut |C(G,P)|, directed entries */
+    uint64_t weighted_directed_edge_cut;
+    uint64_t max_local_cut;              /* max over parts of outgoing + incoming */
+    uint64_t weighted_max_local_cut;
+    double avg_local_cut;
+    double weighted_avg_local_cut;
+    double vertex_avg;                   /* n / parts */
+    uint64_t min_vertices, max_vertices;
+    double vertex_imbalance;             /* max / avg */
+    double vertex_max_deviation;         /* max |part - avg| / avg */
+    double edge_set_avg;                 /* (m + directed cut) / parts */
+    uint64_t min_edge_set, max_edge_set; /* internal + outgoing + incoming */
+    double edge_set_imbalance;
+    double edge_set_max_deviation;
+} gp_analysis;
+
+gp_status gp_analyze(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts, gp_part_stats* per_part,
+                     gp_analysis* summary);
 
 /* Kernel launches issued by this context so far (all of them are the
  * library's own sm_100a kernels). */

@@ -12,7 +12,7 @@ import pytest
 import horkxg_b200 as hb
 import pyoracle as O
 from horkxg_b200 import graphs
-from helpers import goldens, csr_from_rows, weighted_stress
+from helpers import goldens, csr_from_rows, symmetric_rows, weighted_stress
 from test_oracle import EXCHANGE, REPAIR, contraction_fixture, hub_path_259
 
 pytestmark = pytest.mark.gpu
@@ -293,6 +293,49 @@ def test_initial_partition_rejections(ctx):
     assert e.value.status == hb.GP_EOVERFLOW
 
 
+# --- initial partition on the golden graphs' coarsest levels: the oracle
+# replays the recursion on the device's own FP32 vectors, so the split rules
+# (sort by (x, id), prefix, boundary clamps; initial_partition_gpu.cu:230-248)
+# and the task bookkeeping must give identical labels; every traced vector is
+# within the diffusion tolerance of the FP64 oracle on the same task.
+COARSEST_CASES = [("grid2d_256", 4), ("grid3d_24", 8), ("rmat14", 32), ("rmat16", 32), ("rgg_20k", 8)]
+
+
+@pytest.mark.parametrize("small", [True, False], ids=["cluster", "cooperative"])
+@pytest.mark.parametrize("name,k", COARSEST_CASES)
+def test_initial_partition_splits_match_oracle(ctx, name, k, small):
+    _, _, g = file_graph(name)
+    coff, cnbr, cew, cvw, _ = ctx.coarsen(g, parts=k)[-1]
+    cg = hb.HostGraph(coff, cnbr, cew, cvw, index64=True)
+    og = O.Graph(coff, cnbr, cew, cvw)
+    ctx.set_small_diffusion(small)
+    try:
+        for seed in (0, 1, 2):
+            labels, trace = ctx.initial_partition_trace(cg, k, 1.03, seed)
+            assert trace.shape[0] == len(hb.plan_depths(k))
+            assert np.array_equal(labels, ctx.initial_partition(cg, k, 1.03, seed))
+            olabels, err = O.initial_partition_replay(og, k, trace, 1.03, seed)
+            assert np.array_equal(labels, olabels)
+            assert err <= DIFFUSION_TOL, err
+    finally:
+        ctx.set_small_diffusion(True)
+
+
+# --- the whole pipeline in deterministic mode equals the oracle's pipeline
+# started from the device's coarsest labels: the refine schedule
+# (refine.cu:602-606), projections and every refined level
+@pytest.mark.parametrize("name,k,seed", [("rmat14", 32, 0), ("grid2d_256", 4, 0), ("rgg_20k", 8, 1),
+                                         ("grid3d_24", 8, 2)])
+def test_pipeline_matches_oracle_from_device_initial_partition(ctx, name, k, seed):
+    off, idx, g = file_graph(name)
+    coff, cnbr, cew, cvw, _ = ctx.coarsen(g, parts=k, seed=seed)[-1]
+    init = ctx.initial_partition(hb.HostGraph(coff, cnbr, cew, cvw, index64=True), k, 1.03, seed)
+    labels, rep = ctx.partition(g, parts=k, seed=seed, deterministic=1)
+    olabels, ocut = O.partition_from(O.Graph(off, idx), k, init, 1.03, seed)
+    assert rep.cut == ocut
+    assert np.array_equal(labels, olabels)
+
+
 # --- refinement: deterministic mode is bit-exact with the oracle
 def refine_both(ctx, off, nbr, ew, vw, labels, k, width=hb.STANDARD):
     g = hb.HostGraph(off, nbr, ew, vw, width=width, index64=True)
@@ -363,6 +406,44 @@ def test_partition_big_width_matches_standard_hierarchy(ctx):
     a, _ = ctx.partition(gs, parts=8, deterministic=1)
     b, _ = ctx.partition(gb, parts=8, deterministic=1)
     assert np.array_equal(a, b)
+
+
+# --- refinement gain range (validate_refinement_gain_range, refine.cu:346-383)
+def test_refinement_gain_range_rejection(ctx):
+    off, nbr, _ = csr_from_rows(symmetric_rows(4, [(0, 1), (1, 2), (2, 3)]))
+    labels = np.array([0, 0, 1, 1], np.int32)
+    heavy = hb.HostGraph(off, nbr, np.full(len(nbr), 1 << 61, np.uint64), width=hb.BIG, index64=True)
+    for call in (lambda: ctx.refine(heavy, labels, 2), lambda: ctx.partition(heavy, parts=2)):
+        with pytest.raises(hb.PartitionError) as e:
+            call()
+        assert e.value.status == hb.GP_EOVERFLOW and "gain range" in str(e.value)
+    # a directed total of 1.5 * 2^61 stays below INT64_MAX / 2
+    light = hb.HostGraph(off, nbr, np.full(len(nbr), 1 << 59, np.uint64), width=hb.BIG, index64=True)
+    lab, st = ctx.refine(light, labels, 2)
+    assert st.final_cut <= st.initial_cut
+
+
+# --- --verify: the coarsening step checks of validate_coarsening_step
+# (coarsen.cu:1835-1902) run on every level and change nothing
+@pytest.mark.parametrize("name,k,width", [("rmat14", 32, "standard"), ("grid2d_256", 4, "standard"),
+                                          ("grid3d_24", 8, "big")])
+def test_verify_mode_checks_every_level(ctx, name, k, width):
+    off, idx, g = file_graph(name, width)
+    a, ra = ctx.partition(g, parts=k, deterministic=1)
+    b, rb = ctx.partition(g, parts=k, deterministic=1, verify=1)
+    assert np.array_equal(a, b) and ra.cut == rb.cut and ra.levels == rb.levels
+
+
+def test_verify_driver_prints_layer_checks(ctx, tmp_path):
+    indptr, indices = graphs.by_name("grid2d_256")
+    out = tmp_path / "labels.bin"
+    r = subprocess.run([str(hb.BIN / "gpart_partition_standard"), str(indptr), str(indices), "4", str(out),
+                        "1.03", "0", "--verify"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = re.findall(r"^ml_layer_verify level=(\d+) map=ok weights=ok csr=ok projection_cut=ok$", r.stdout, re.M)
+    _, _, g = file_graph("grid2d_256")
+    levels = ctx.partition(g, parts=4).levels      # the hierarchy does not depend on the refinement
+    assert [int(x) for x in lines] == list(range(levels - 1))
 
 
 def test_invalid_input_errors(ctx):
