@@ -82,6 +82,11 @@ class Analysis(ctypes.Structure):
                 ("edge_set_max_deviation", ctypes.c_double)]
 
 
+class SymmetrizeInfo(ctypes.Structure):
+    _fields_ = [("self_loops_removed", ctypes.c_int64), ("unique_undirected_edges", ctypes.c_int64),
+                ("output_directed_edges", ctypes.c_int64)]
+
+
 class RefineStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_int32), ("proposals", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
                 ("initial_cut", ctypes.c_uint64), ("final_cut", ctypes.c_uint64),
@@ -92,8 +97,8 @@ class RefineStats(ctypes.Structure):
 EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_error", "gp_partition_capacity",
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
-           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
-           "gp_initial_partition_static", "gp_initial_partition_trace", "gp_analyze", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
+           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_set_hub_tables", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
+           "gp_initial_partition_static", "gp_initial_partition_trace", "gp_analyze", "gp_symmetrize", "gp_generate_rmat", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
            "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
            "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
 
@@ -128,6 +133,9 @@ def lib() -> ctypes.CDLL:
         L.gp_refine.argtypes = [vp, P(GraphDesc), vp, i32, dbl, i32, i32, P(RefineStats)]
         L.gp_cut.argtypes = [vp, P(GraphDesc), vp, i32, P(ctypes.c_uint64), vp]
         L.gp_analyze.argtypes = [vp, P(GraphDesc), vp, i32, P(PartStats), P(Analysis)]
+        L.gp_symmetrize.argtypes = [vp, P(GraphDesc), vp, vp, i32, i64, P(SymmetrizeInfo)]
+        L.gp_generate_rmat.argtypes = [vp, i32, i32, dbl, dbl, dbl, ctypes.c_uint64, i32, vp, vp, i32, i64,
+                                       P(SymmetrizeInfo)]
         L.gp_launch_count.argtypes = [vp]
         L.gp_launch_count.restype = ctypes.c_uint64
         L.gp_sync_count.argtypes = [vp]
@@ -135,6 +143,7 @@ def lib() -> ctypes.CDLL:
         L.gp_ctx_set_sync_mode.argtypes = [vp, i32]
         L.gp_ctx_set_device_share.argtypes = [vp, i32]
         L.gp_ctx_set_small_diffusion.argtypes = [vp, i32]
+        L.gp_ctx_set_hub_tables.argtypes = [vp, i32]
         L.gp_ctx_stream.argtypes = [vp]
         L.gp_ctx_stream.restype = vp
         L.gp_profile_enable.argtypes = [vp, i32]
@@ -393,6 +402,10 @@ class Context:
         """One-block diffusion for small coarsest graphs (same values)."""
         self._check(lib().gp_ctx_set_small_diffusion(self._h, int(enable)))
 
+    def set_hub_tables(self, on_chip: bool):
+        """On-chip hub hash tables where they fit (same hierarchy)."""
+        self._check(lib().gp_ctx_set_hub_tables(self._h, int(on_chip)))
+
     def set_device_share(self, share: int):
         """Contexts expected to run at once on the device (grid sizing only)."""
         self._check(lib().gp_ctx_set_device_share(self._h, int(share)))
@@ -570,3 +583,25 @@ class Context:
         self._check(lib().gp_analyze(self._h, ctypes.byref(d), labels.ctypes.data, parts, st, ctypes.byref(a)))
         per = {f: np.array([getattr(x, f) for x in st], np.uint64) for f, _ in PartStats._fields_}
         return per, {f: getattr(a, f) for f, _ in Analysis._fields_ if f != "reserved"}
+
+    def symmetrize(self, g: HostGraph, neighbor_bytes: int = 8):
+        """The reference symmetriser's output on the GPU: (int64 offsets,
+        neighbours (int64 or int32), SymmetrizeInfo)."""
+        off = np.zeros(g.n + 1, np.int64)
+        nbr = np.zeros(max(2 * g.m, 1), np.int64 if neighbor_bytes == 8 else np.int32)
+        info = SymmetrizeInfo()
+        d = g.desc()
+        self._check(lib().gp_symmetrize(self._h, ctypes.byref(d), off.ctypes.data, nbr.ctypes.data, neighbor_bytes,
+                                        2 * g.m, ctypes.byref(info)))
+        return off, nbr[:info.output_directed_edges].copy(), info
+
+    def generate_rmat(self, scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+                      seed: int = 1, neighbor_bytes: int = 8):
+        """R-MAT generated and symmetrised on the GPU, copied to the host."""
+        n = 1 << scale
+        off = np.zeros(n + 1, np.int64)
+        nbr = np.zeros(2 * n * edge_factor, np.int64 if neighbor_bytes == 8 else np.int32)
+        info = SymmetrizeInfo()
+        self._check(lib().gp_generate_rmat(self._h, scale, edge_factor, a, b, c, seed, HOST, off.ctypes.data,
+                                           nbr.ctypes.data, neighbor_bytes, len(nbr), ctypes.byref(info)))
+        return off, nbr[:info.output_directed_edges].copy(), info

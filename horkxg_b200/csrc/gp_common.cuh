@@ -88,6 +88,9 @@ struct Device {
     // Small coarsest graphs take the one-block diffusion (same values as the
     // cooperative kernel); off only to compare the two.
     bool small_diffusion = true;
+    // SCLP affinity of hubs with on-chip tables where they fit (same
+    // results as the global tables); off only to compare the two.
+    bool hub_chip = true;
     int grid_limit(int per_sm) const { return std::max(sms / 2, sms * per_sm / std::max(1, share)); }
     u32* err = nullptr;         // device error word
     void* pinned = nullptr;     // small pinned host staging area

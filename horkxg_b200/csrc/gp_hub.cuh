@@ -190,6 +190,114 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(
 
 struct HubPartial { u64 current, best, tie; };
 
+// ---------------------------------------------------------------------------
+// SCLP affinity of hubs whose table fits in one CTA's shared memory (up to
+// ~9.4K edges): one CTA per hub does the inserts, the candidate scan and the
+// decode in one launch, so these tables never reach global memory and need
+// neither a clearing memset nor a separate candidate pass.  8-byte slots
+// (cluster + 1, 32-bit sum) claimed by one 64-bit CAS, as HubSlot32: used on
+// levels whose total edge weight fits 32 bits.  Larger hubs keep the chunked
+// global tables: one CTA walking 10^4-10^5 edges would be a long chain of
+// dependent loads, where the chunks spread a hub over many CTAs.
+// ---------------------------------------------------------------------------
+constexpr int kHubSmemThreads = 512;
+constexpr int kHubSmemWarps = kHubSmemThreads / 32;
+constexpr int kHubSmemSlots = 12288;        // 96 KB, two CTAs per SM
+
+// Table slots for a hub of `degree` edges: at least 1.3x the degree (a hub
+// has at most `degree` distinct neighbour clusters), whole 32-slot lines.
+__host__ __device__ inline i64 hub_smem_slots(i64 degree) {
+    const i64 want = degree + (degree * 3 + 9) / 10;
+    return (want + 31) / 32 * 32;
+}
+
+template <typename O, typename W>
+__global__ void __launch_bounds__(kHubSmemThreads) hub_smem_kernel(
+    const i32* __restrict__ hub_ids, const O* __restrict__ off, const i32* __restrict__ nbr,
+    const W* __restrict__ ew, const W* __restrict__ vw, const i32* __restrict__ clusters,
+    const u64* __restrict__ cw, RoundParams p, SclpOut out) {
+    extern __shared__ unsigned long long table[];   // kHubSmemSlots at most
+    __shared__ u64 red[3][kHubSmemWarps];
+    const i32 v = hub_ids[blockIdx.x];
+    const i32 source = clusters[v];
+    if (role_blocked(source, p)) {
+        if (threadIdx.x == 0) out.target[v] = kInvalid;
+        return;
+    }
+    const i64 b = off[v], end = off[v + 1];
+    const u32 size = static_cast<u32>(hub_smem_slots(end - b));
+    for (u32 s = threadIdx.x; s < size; s += kHubSmemThreads) table[s] = 0ULL;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (i64 base = b; base < end; base += kHubSmemThreads) {
+        const i64 e = base + threadIdx.x;
+        i32 c = -1;
+        u64 w = 0;
+        if (e < end) {
+            const i32 u = nbr[e];
+            if (u != v) {
+                c = clusters[u];
+                w = static_cast<u64>(weight_at(ew, e));
+            }
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        u64 sum = 0;
+        if (ew == nullptr) {
+            sum = static_cast<u64>(__popc(peers));
+        } else {
+#pragma unroll
+            for (int s = 0; s < 32; ++s) {
+                const u64 pw = __shfl_sync(0xffffffffu, w, s);
+                if (peers & (1u << s)) sum += pw;
+            }
+        }
+        if (c >= 0 && lane == __ffs(peers) - 1) {
+            const u32 key = static_cast<u32>(c) + 1;
+            const unsigned long long fresh = (static_cast<unsigned long long>(static_cast<u32>(sum)) << 32) | key;
+            u32 slot = slot_of(c, size);
+            // at most size probes: the table has more slots than distinct keys
+            for (u32 probe = 0; probe < size; ++probe) {
+                const unsigned long long found = atomicCAS(&table[slot], 0ULL, fresh);
+                if (found == 0ULL) break;
+                if (static_cast<u32>(found) == key) {
+                    atomicAdd(reinterpret_cast<u32*>(&table[slot]) + 1, static_cast<u32>(sum));
+                    break;
+                }
+                if (++slot == size) slot = 0;
+            }
+        }
+    }
+    __syncthreads();
+    u64 current = 0, best = 0, tie = 0;
+    for (u32 s = threadIdx.x; s < size; s += kHubSmemThreads) {
+        const unsigned long long x = table[s];
+        const u32 key = static_cast<u32>(x);
+        if (key) slot_candidate(static_cast<i32>(key - 1), x >> 32, static_cast<u32>(v), source, p, current, best, tie);
+    }
+    group_reduce(current, best, tie, 32, 0xffffffffu);
+    const int warp = threadIdx.x >> 5;
+    if (lane == 0) { red[0][warp] = current; red[1][warp] = best; red[2][warp] = tie; }
+    __syncthreads();
+    if (warp == 0) {
+        current = lane < kHubSmemWarps ? red[0][lane] : 0;
+        best = lane < kHubSmemWarps ? red[1][lane] : 0;
+        tie = lane < kHubSmemWarps ? red[2][lane] : 0;
+        group_reduce(current, best, tie, 32, 0xffffffffu);
+        if (lane == 0) decode_and_write(v, source, current, best, tie, p, vw, cw, out);
+    }
+}
+
+// Degree and first edge of every hub (for the host's split of the hubs into
+// on-chip classes and global-table hubs, once per level).
+template <typename O>
+__global__ void hub_extent_kernel(i64 count, const i32* __restrict__ hubs, const O* __restrict__ off, i64* out) {
+    const i64 h = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (h >= count) return;
+    const i32 v = hubs[h];
+    out[2 * h] = static_cast<i64>(off[v]);
+    out[2 * h + 1] = static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]);
+}
+
 // Profiling only: the work an affinity pass over `list` really does, since
 // vertices (and hubs) whose own cluster is not a mover are skipped.  out[0]
 // counts the processed vertices, out[1] their edges, out[2] the slots of

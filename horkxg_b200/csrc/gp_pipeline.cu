@@ -28,6 +28,7 @@
 #include "gp_refine.cuh"
 #include "gp_hub.cuh"
 #include "gp_analyze.cuh"
+#include "gp_symmetrize.cuh"
 
 namespace gp {
 
@@ -83,6 +84,15 @@ struct DGraph {
         Buf<i32> list;
         Buf<Chunk> chunk;
         Buf<i64> chunk_begin;   // per hub, count + 1 entries
+        // SCLP affinity split (hub_split): the hubs whose table fits one
+        // CTA's shared memory (chip_ids), and the hubs that keep global
+        // tables, with their own chunk list (Chunk::hub indexes global_list)
+        bool split_built = false;
+        Buf<i32> chip_ids;
+        i64 chip_count = 0;
+        i64 global_count = 0, global_chunks = 0;
+        Buf<i32> global_list;
+        Buf<Chunk> global_chunk;
     };
     mutable Hubs hubs;
     // rows free of duplicate neighbours: 1 yes, 0 no, -1 not yet checked
@@ -123,6 +133,56 @@ const typename DGraph<T>::Hubs& hub_index(Device& d, const DGraph<T>& g, i64 kno
                                 d.stream));
     }
     h.built = true;
+    return h;
+}
+
+// Splits a level's hubs (once) into those of hub_smem_kernel and those that
+// keep the global tables.
+template <typename T>
+const typename DGraph<T>::Hubs& hub_split(Device& d, const DGraph<T>& g) {
+    using O = typename T::O;
+    const auto& hubs = hub_index(d, g);
+    auto& h = g.hubs;
+    if (h.split_built) return h;
+    std::vector<i64> ext(static_cast<size_t>(2 * hubs.count));
+    std::vector<i32> ids(static_cast<size_t>(hubs.count));
+    if (hubs.count) {
+        Buf<i64> dev_ext(d, ext.size());
+        launch(d, "hub_extent_kernel", hub_extent_kernel<O>, blocks_for(hubs.count, kThreads), kThreads, 0,
+               hubs.count, hubs.list.get(), g.off.get(), dev_ext.get());
+        GP_LAUNCH();
+        to_host(d, ext.data(), dev_ext.get(), ext.size());
+        to_host(d, ids.data(), hubs.list.get(), ids.size());
+        d.sync();
+    }
+    std::vector<i32> chip, glob;
+    std::vector<Chunk> chunks;
+    for (i64 i = 0; i < hubs.count; ++i) {
+        const i64 begin = ext[2 * i], degree = ext[2 * i + 1];
+        if (hub_smem_slots(degree) <= kHubSmemSlots) {
+            chip.push_back(ids[i]);
+            continue;
+        }
+        const i32 gi = static_cast<i32>(glob.size());
+        glob.push_back(ids[i]);
+        for (i64 e = begin; e < begin + degree; e += kChunkEdges)
+            chunks.push_back({ids[i], gi, e, std::min(e + kChunkEdges, begin + degree)});
+    }
+    h.chip_count = static_cast<i64>(chip.size());
+    if (!chip.empty()) {
+        h.chip_ids = Buf<i32>(d, chip.size());
+        to_device(d, h.chip_ids.get(), chip.data(), chip.size());
+    }
+    h.global_count = static_cast<i64>(glob.size());
+    h.global_chunks = static_cast<i64>(chunks.size());
+    if (!glob.empty()) {
+        h.global_list = Buf<i32>(d, glob.size());
+        h.global_chunk = Buf<Chunk>(d, chunks.size());
+        to_device(d, h.global_list.get(), glob.data(), glob.size());
+        to_device(d, h.global_chunk.get(), chunks.data(), chunks.size());
+    }
+    d.sync();   // host vectors go out of scope
+    h.split_built = true;
     return h;
 }
 
@@ -328,17 +388,27 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     const bool direct_ok = unique_rows(d, g);
     // global hash tables for hubs
     if (hubs.count != static_cast<i64>(cnt[5])) fail(GP_ERUNTIME, "hub index disagrees with degree classes");
+    // Hubs whose table fits on chip (32-bit sums) run hub_smem_kernel; the
+    // others keep per-hub tables in global memory.
+    const bool chip = sum32 && hubs.count > 0 && d.hub_chip;
+    if (chip) hub_split(d, g);
+    const i64 gcount = chip ? hubs.global_count : hubs.count;
+    const i64 gchunks = chip ? hubs.global_chunks : hubs.chunks;
+    const i32* glist = chip ? hubs.global_list.get() : hubs.list.get();
+    const Chunk* gchunk = chip ? hubs.global_chunk.get() : hubs.chunk.get();
     i64 table_total = 0;
     if (hubs.count > 0) {
-        w.table_off.ensure(d, static_cast<size_t>(hubs.count) + 1);
-        exclusive_scan<i64>(d, HubTableSize<O>{hubs.list.get(), off, hubs.count}, w.table_off.get(),
-                            hubs.count + 1, reinterpret_cast<i64*>(sc + 4));
-        fetch(d, &table_total, reinterpret_cast<i64*>(sc + 4), 1);
+        if (gcount > 0) {
+            w.table_off.ensure(d, static_cast<size_t>(gcount) + 1);
+            exclusive_scan<i64>(d, HubTableSize<O>{glist, off, gcount}, w.table_off.get(), gcount + 1,
+                                reinterpret_cast<i64*>(sc + 4));
+            fetch(d, &table_total, reinterpret_cast<i64*>(sc + 4), 1);
+            w.table.ensure(d, static_cast<size_t>(table_total));
+            GP_CUDA(cudaMemsetAsync(w.table.get(), 0, table_total * (sum32 ? sizeof(HubSlot32) : sizeof(HubSlot)),
+                                    d.stream));
+        }
+        // the identity rounds' hub_direct_kernel writes one partial per chunk of every hub
         w.partials.ensure(d, static_cast<size_t>(std::max<i64>(table_total / kSlotTile, hubs.chunks)));
-        w.table.ensure(d, static_cast<size_t>(table_total));
-
-        GP_CUDA(cudaMemsetAsync(w.table.get(), 0, table_total * (sum32 ? sizeof(HubSlot32) : sizeof(HubSlot)),
-                                d.stream));
     }
 
     trace().mark(d, "agg.hub_tables", level);
@@ -357,6 +427,7 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
     // weight and cluster gather (none at round 0); a skipped vertex reads its
     // cluster and writes an empty proposal.
     u64 work[kClasses][3] = {};
+    u64 gwork[3] = {};   // the same for the hubs with global tables
     auto affinity_bytes = [&](int c, bool identity) {
         const double v = static_cast<double>(work[c][0]), e = static_cast<double>(work[c][1]);
         return v * (2 * sizeof(O) + 4 + 4 + 8 + 4 + 8 + 4 + 8) + (static_cast<double>(cnt[c]) - v) * 8 +
@@ -371,6 +442,15 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
                     launch(d, "role_work_kernel", role_work_kernel<O>, stride_grid(d, cnt[c]), kThreads, 0,
                            static_cast<i64>(cnt[c]), class_list(c), off, clusters, p, cw_dev.get() + 3 * c);
             fetch(d, &work[0][0], cw_dev.get(), 3 * kClasses);
+            if (chip && gcount) {
+                Buf<u64> gw(d, 3);
+                gw.zero(d);
+                launch(d, "role_work_kernel", role_work_kernel<O>, stride_grid(d, gcount), kThreads, 0, gcount, glist,
+                       off, clusters, p, gw.get());
+                fetch(d, gwork, gw.get(), 3);
+            } else {
+                for (int j = 0; j < 3; ++j) gwork[j] = work[5][j];
+            }
             d.prof_bytes("affinity_small_kernel", affinity_bytes(1, p.identity) + affinity_bytes(2, p.identity));
             if (!(p.identity && direct_ok)) {   // the direct kernels of identity rounds carry no model
                 d.prof_bytes("affinity_warp_hash_kernel", affinity_bytes(3, p.identity));
@@ -409,25 +489,40 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
         if (cnt[4])
             launch(d, "affinity_block_hash_kernel", affinity_block_hash_kernel<O, W>, static_cast<int>(cnt[4]), kThreads, kLargeSlots * 12, 
                 cnt[4], class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
-        if (cnt[5]) {
-            // chunk records of all hubs; neighbour, weight and cluster of
-            // each edge of the hubs that are not skipped; the slots of their
-            // tables for the candidate pass
-            d.prof_bytes("hub_insert_kernel", static_cast<double>(work[5][1]) * (4 + 4 + (ew ? sizeof(W) : 0)) +
-                                                  static_cast<double>(hubs.chunks) * sizeof(Chunk));
+        if (cnt[5] && chip) {
+            // per processed on-chip hub: its offsets, cluster and proposal
+            // writes; per edge its neighbour, weight and cluster gather
+            const double chip_edges = static_cast<double>(work[5][1] - gwork[1]);
+            const double chip_hubs = static_cast<double>(work[5][0] - gwork[0]);
+            d.prof_bytes("hub_smem_kernel", chip_hubs * (2 * sizeof(O) + 4 + 4 + 8 + 4 + 8) +
+                                                chip_edges * (4 + 4 + (ew ? sizeof(W) : 0)));
+            if (hubs.chip_count) {
+                const size_t smem = static_cast<size_t>(kHubSmemSlots) * sizeof(unsigned long long);
+                GP_CUDA(cudaFuncSetAttribute(hub_smem_kernel<O, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+                launch(d, "hub_smem_kernel", hub_smem_kernel<O, W>, static_cast<int>(hubs.chip_count),
+                       kHubSmemThreads, smem, hubs.chip_ids.get(), off, nbr, ew, vw, clusters, cw, p, so);
+            }
+        }
+        if (cnt[5] && gcount) {
+            // chunk records of the global-table hubs; neighbour, weight and
+            // cluster of each edge of the hubs that are not skipped; the
+            // slots of their tables for the candidate pass
+            d.prof_bytes("hub_insert_kernel", static_cast<double>(gwork[1]) * (4 + 4 + (ew ? sizeof(W) : 0)) +
+                                                  static_cast<double>(gchunks) * sizeof(Chunk));
             auto hub_tables = [&](auto* table) {
                 using S = std::remove_pointer_t<decltype(table)>;
-                d.prof_bytes("hub_candidates_kernel", static_cast<double>(work[5][2]) * sizeof(S));
-                launch(d, "hub_insert_kernel", hub_insert_kernel<O, W, S>, static_cast<int>(hubs.chunks), kThreads, 0,
-                       hubs.chunk.get(), nbr, ew, clusters, p, w.table_off.get(), table, d.err);
+                d.prof_bytes("hub_candidates_kernel", static_cast<double>(gwork[2]) * sizeof(S));
+                launch(d, "hub_insert_kernel", hub_insert_kernel<O, W, S>, static_cast<int>(gchunks), kThreads, 0,
+                       gchunk, nbr, ew, clusters, p, w.table_off.get(), table, d.err);
                 launch(d, "hub_candidates_kernel", hub_candidates_kernel<W, S>,
-                       static_cast<int>(table_total / kSlotTile), kThreads, 0, hubs.count, hubs.list.get(),
-                       w.table_off.get(), table, clusters, p, w.partials.get(), i64{0});
+                       static_cast<int>(table_total / kSlotTile), kThreads, 0, gcount, glist, w.table_off.get(), table,
+                       clusters, p, w.partials.get(), i64{0});
             };
             if (sum32) hub_tables(reinterpret_cast<HubSlot32*>(w.table.get()));
             else hub_tables(w.table.get());
-            launch(d, "hub_finalize_kernel", hub_finalize_kernel<W>, blocks_for(hubs.count, kThreads), kThreads, 0,
-                   hubs.count, hubs.list.get(), w.table_off.get(), w.partials.get(), clusters, vw, cw, p, so);
+            launch(d, "hub_finalize_kernel", hub_finalize_kernel<W>, blocks_for(gcount, kThreads), kThreads, 0, gcount,
+                   glist, w.table_off.get(), w.partials.get(), clusters, vw, cw, p, so);
         }
         GP_LAUNCH();
     };
@@ -1201,12 +1296,29 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     gp_refine_stats st{};
     w.locks.zero(d);
     w.flags.zero(d);
-    d.prof_bytes("build_cache_kernel", static_cast<double>(n + 1) * sizeof(O) +
-                                           static_cast<double>(g.m) * (4 + 4 + (ew ? sizeof(W) : 0)) +
-                                           static_cast<double>(n) * k * sizeof(C));
-    launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr, ew,
-           labels, k, cache);
     const auto& hubs = hub_index(d, g);
+    double build_bytes = 0;
+    if (d.prof) {
+        // offsets; neighbour, weight and label of every edge of a row below
+        // the hub degree (hub rows are built by the chunked kernel); the
+        // cache rows written
+        i64 hub_edges = 0;
+        if (hubs.count) {
+            std::vector<i64> ext(static_cast<size_t>(2 * hubs.count));
+            Buf<i64> dev_ext(d, ext.size());
+            launch(d, "hub_extent_kernel", hub_extent_kernel<O>, blocks_for(hubs.count, kThreads), kThreads, 0,
+                   hubs.count, hubs.list.get(), off, dev_ext.get());
+            to_host(d, ext.data(), dev_ext.get(), ext.size());
+            d.sync();
+            for (i64 i = 0; i < hubs.count; ++i) hub_edges += ext[2 * i + 1];
+        }
+        build_bytes = static_cast<double>(n + 1) * sizeof(O) +
+                      static_cast<double>(g.m - hub_edges) * (4 + 4 + (ew ? sizeof(W) : 0)) +
+                      static_cast<double>(n - hubs.count) * k * sizeof(C);
+        d.prof_bytes("build_cache_kernel", build_bytes);
+    }
+    launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 8), kThreads, 0, n, off, nbr, ew,
+           labels, k, cache);
     Buf<long long> hub_corr;
     if (hubs.count) {
         launch(d, "zero_hub_rows_kernel", zero_hub_rows_kernel<C>, blocks_for(hubs.count * k, kThreads), kThreads, 0,
@@ -1241,7 +1353,8 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     struct Stats { RefineCounters c; u64 pw[32]; };
     static_assert(sizeof(Stats) <= Device::kPinnedBytes, "stats fit the pinned staging buffer");
     auto build_cache = [&]() {
-        launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 32), kThreads, 0, n, off, nbr,
+        d.prof_bytes("build_cache_kernel", build_bytes);
+        launch(d, "build_cache_kernel", build_cache_kernel<O, W, C>, stride_grid(d, n * 8), kThreads, 0, n, off, nbr,
                ew, labels, k, cache);
         if (hubs.count) {
             launch(d, "zero_hub_rows_kernel", zero_hub_rows_kernel<C>, blocks_for(hubs.count * k, kThreads), kThreads,
@@ -1408,6 +1521,18 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         d.prof_bytes("lp_proposals_kernel", static_cast<double>(n) * (k * sizeof(C) + 4 + 1 + 4 + 8));
         launch(d, "lp_proposals_kernel", lp_proposals_kernel<C>, blocks_for(n, kThreads), kThreads, 0, n, cache, labels, k,
                filter, max_edge_weight, w.locks.get(), w.targets.get(), w.gains.get(), w.props.get(), w.list.get(), ctr);
+        if (d.prof) {
+            // per proposer its list entry, offsets, record and flag; per edge
+            // of a proposer below the hub degree its neighbour, weight and
+            // the neighbour's 16-byte proposal record (filter_degree)
+            RefineCounters pc{};
+            launch(d, "filter_degree_kernel", filter_degree_kernel<O>, stride_grid(d, n), kThreads, 0, w.list.get(),
+                   ctr, off, ctr);
+            fetch(d, &pc, ctr, 1);
+            d.prof_bytes("priority_filter_kernel",
+                         static_cast<double>(pc.proposers) * (4 + 2 * sizeof(O) + sizeof(PropRec) + 1) +
+                             static_cast<double>(pc.filter_degree) * (4 + (ew ? sizeof(W) : 0) + sizeof(PropRec)));
+        }
         launch(d, "priority_filter_kernel", priority_filter_kernel<O, W>, stride_grid(d, n * 32), kThreads, 0,
                w.list.get(), ctr, off, nbr, ew, w.props.get(), w.flags.get(), w.movers.get(), ctr);
         if (hubs.count) {
@@ -1765,6 +1890,70 @@ void analyze_parts(Device& d, const DGraph<T>& g, const i32* labels, int parts, 
     fetch(d, out.data(), acc.get(), cells);
 }
 
+// Sorts the directed keys (sentinels last), keeps the first of each run and
+// writes the symmetric CSR: offsets (n + 1, device) and neighbours (device,
+// `capacity` entries).  Returns the number of output entries; when it exceeds
+// `capacity` nothing is written.
+template <typename N>
+i64 symmetrize_keys(Device& d, Buf<u64>& keys, Buf<u64>& alt, i64 total_keys, i64 valid, i64 n, int bits,
+                    i64* out_off, N* out_nbr, i64 capacity, bool sorted) {
+    if (!sorted) radix_sort<u64, i32>(d, keys.get(), nullptr, alt.get(), nullptr, total_keys, 0, 2 * bits);
+    Buf<i64> rank(d, static_cast<size_t>(std::max<i64>(valid, 1))), tot(d, 1);
+    exclusive_scan<i64>(d, SymHead{keys.get(), valid}, rank.get(), valid, tot.get());
+    i64 out_m = 0;
+    fetch(d, &out_m, tot.get(), 1);
+    if (out_m > capacity) return out_m;
+    Buf<i64> degree(d, static_cast<size_t>(std::max<i64>(n, 1)));
+    degree.zero(d);
+    if (valid)
+        launch(d, "sym_compact_kernel", sym_compact_kernel<N>, stride_grid(d, valid), kThreads, 0, valid, keys.get(),
+               rank.get(), bits, out_nbr, degree.get());
+    exclusive_scan<i64>(d, ArrayInput<i64>{degree.get()}, out_off, n, out_off + n);
+    GP_LAUNCH();
+    return out_m;
+}
+
+// The symmetric CSR from 2m directed keys of which `valid` are not
+// sentinels, into the caller's arrays (host or device), with the sizes in
+// `info`; GP_EINVAL when `capacity` is too small.  `sorted`: the keys are
+// sorted already.
+void emit_symmetric(Device& d, Buf<u64>& keys, Buf<u64>& alt, i64 total_keys, i64 valid, i64 n, int bits, u64 self,
+                    bool on_dev, i64* offsets_out, void* neighbors_out, int neighbor_bytes, i64 capacity,
+                    gp_symmetrize_info* info, bool sorted = false);
+
+inline int symmetrize_bits(i64 n) { return std::max(1, bit_width_u64(static_cast<u64>(std::max<i64>(n, 1) - 1))); }
+
+void emit_symmetric(Device& d, Buf<u64>& keys, Buf<u64>& alt, i64 total_keys, i64 valid, i64 n, int bits, u64 self,
+                    bool on_dev, i64* offsets_out, void* neighbors_out, int neighbor_bytes, i64 capacity,
+                    gp_symmetrize_info* info, bool sorted) {
+    Buf<i64> off_tmp;
+    Buf<unsigned char> nbr_tmp;
+    i64* off_dev = offsets_out;
+    void* nbr_dev = neighbors_out;
+    const i64 cap_dev = on_dev ? capacity : std::min<i64>(capacity, valid);
+    if (!on_dev) {
+        off_tmp = Buf<i64>(d, static_cast<size_t>(n) + 1);
+        nbr_tmp = Buf<unsigned char>(d, static_cast<size_t>(std::max<i64>(cap_dev, 1)) * neighbor_bytes);
+        off_dev = off_tmp.get();
+        nbr_dev = nbr_tmp.get();
+    }
+    const i64 out_m = neighbor_bytes == 8
+                          ? symmetrize_keys<i64>(d, keys, alt, total_keys, valid, n, bits, off_dev,
+                                                 static_cast<i64*>(nbr_dev), cap_dev, sorted)
+                          : symmetrize_keys<i32>(d, keys, alt, total_keys, valid, n, bits, off_dev,
+                                                 static_cast<i32*>(nbr_dev), cap_dev, sorted);
+    if (info) *info = gp_symmetrize_info{static_cast<int64_t>(self), out_m / 2, out_m};
+    if (out_m > capacity)
+        fail(GP_EINVAL, "neighbor capacity " + std::to_string(capacity) + " is below the " + std::to_string(out_m) +
+                            " entries of the symmetric CSR");
+    if (!on_dev) {
+        to_host(d, offsets_out, off_dev, static_cast<size_t>(n) + 1);
+        GP_CUDA(cudaMemcpyAsync(neighbors_out, nbr_dev, static_cast<size_t>(out_m) * neighbor_bytes,
+                                cudaMemcpyDeviceToHost, d.stream));
+    }
+    d.sync();
+}
+
 template <typename T>
 void host_level_copy(Device& d, const DGraph<T>& g, const i32* map, i64 map_n, std::vector<i64>& off,
                      std::vector<i32>& nbr, std::vector<u64>& ew, std::vector<u64>& vw, std::vector<i32>& mp) {
@@ -2087,6 +2276,12 @@ gp_status gp_ctx_set_device_share(gp_ctx* ctx, int share) {
 gp_status gp_ctx_set_small_diffusion(gp_ctx* ctx, int enable) {
     if (!ctx) return GP_EINVAL;
     ctx->dev.small_diffusion = enable != 0;
+    return GP_OK;
+}
+
+gp_status gp_ctx_set_hub_tables(gp_ctx* ctx, int on_chip) {
+    if (!ctx) return GP_EINVAL;
+    ctx->dev.hub_chip = on_chip != 0;
     return GP_OK;
 }
 
@@ -2656,6 +2851,85 @@ gp_status gp_analyze(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, 
                                                 deviation(static_cast<double>(a.min_edge_set), a.edge_set_avg));
             if (summary) *summary = a;
         });
+    });
+}
+
+gp_status gp_symmetrize(gp_ctx* ctx, const gp_graph* graph, int64_t* offsets_out, void* neighbors_out,
+                        int32_t neighbor_bytes, int64_t capacity, gp_symmetrize_info* info) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        if (neighbor_bytes != 4 && neighbor_bytes != 8) gp::fail(GP_EINVAL, "neighbor_bytes must be 4 or 8");
+        if (!offsets_out || !neighbors_out || capacity < 0) gp::fail(GP_EINVAL, "null output or negative capacity");
+        with_width(graph, [&](auto tag) {
+            using T = decltype(tag);
+            auto& d = ctx->dev;
+            gp::DGraph<T> g;
+            gp::prepare_graph<T>(d, graph, g, false);
+            const gp::i64 n = g.n, m = g.m;
+            const int bits = gp::symmetrize_bits(n);
+            gp::Buf<gp::u64> keys(d, static_cast<size_t>(std::max<gp::i64>(2 * m, 1)));
+            gp::Buf<gp::u64> alt(d, static_cast<size_t>(std::max<gp::i64>(2 * m, 1)));
+            gp::Buf<gp::u64> loops(d, 1);
+            loops.zero(d);
+            if (m)
+                gp::launch(d, "sym_keys_kernel", gp::sym_keys_kernel<typename T::O>, gp::stride_grid(d, n * 32),
+                           gp::kThreads, 0, n, g.off.get(), g.nbr.get(), bits, keys.get(), loops.get());
+            GP_LAUNCH();
+            gp::u64 self = 0;
+            gp::fetch(d, &self, loops.get(), 1);
+            gp::emit_symmetric(d, keys, alt, 2 * m, 2 * (m - static_cast<gp::i64>(self)), n, bits, self,
+                               graph->memory == GP_MEMORY_DEVICE, offsets_out, neighbors_out, neighbor_bytes, capacity,
+                               info);
+        });
+    });
+}
+
+gp_status gp_generate_rmat(gp_ctx* ctx, int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                           int32_t memory, int64_t* offsets_out, void* neighbors_out, int32_t neighbor_bytes,
+                           int64_t capacity, gp_symmetrize_info* info) {
+    if (!ctx) return GP_EINVAL;
+    return guarded(ctx, [&] {
+        GP_CUDA(cudaSetDevice(ctx->dev.device));
+        if (scale < 1 || scale > 30 || edge_factor < 1 || !(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0))
+            gp::fail(GP_EINVAL, "invalid rmat parameters");
+        if (neighbor_bytes != 4 && neighbor_bytes != 8) gp::fail(GP_EINVAL, "neighbor_bytes must be 4 or 8");
+        if (!offsets_out || !neighbors_out || capacity < 0) gp::fail(GP_EINVAL, "null output or negative capacity");
+        auto& d = ctx->dev;
+        const gp::i64 n = gp::i64{1} << scale;
+        const gp::i64 pairs = n * edge_factor;
+        // the streams and the seeded Fisher-Yates relabelling of the host
+        // generator (horkxg_b200/csrc/gen.cpp, build_rmat)
+        const gp::u64 stream = gp::splitmix64(seed * 0x100000001b3ULL + 0x5851f42d4c957f2dULL);
+        std::vector<gp::u32> perm(static_cast<size_t>(n));
+        for (gp::i64 v = 0; v < n; ++v) perm[v] = static_cast<gp::u32>(v);
+        const gp::u64 pstream = gp::splitmix64(stream ^ 0xa0761d6478bd642fULL);
+        for (gp::i64 v = n - 1; v > 0; --v) {
+            const gp::u64 j = gp::splitmix64(pstream ^ static_cast<gp::u64>(v)) % static_cast<gp::u64>(v + 1);
+            std::swap(perm[v], perm[j]);
+        }
+        gp::Buf<gp::u32> dperm(d, static_cast<size_t>(n));
+        gp::to_device(d, dperm.get(), perm.data(), perm.size());
+        const int bits = gp::symmetrize_bits(n);
+        gp::Buf<gp::u64> keys(d, static_cast<size_t>(2 * pairs)), alt(d, static_cast<size_t>(2 * pairs));
+        gp::launch(d, "rmat_keys_kernel", gp::rmat_keys_kernel, gp::stride_grid(d, pairs), gp::kThreads, 0, pairs,
+                   scale, a, a + b, a + b + c, stream, dperm.get(), bits, keys.get());
+        GP_LAUNCH();
+        d.sync();   // the host permutation goes out of scope
+        // self loops are the pairs whose keys are sentinels: counted from the
+        // sorted keys (they sort last)
+        gp::radix_sort<gp::u64, gp::i32>(d, keys.get(), nullptr, alt.get(), nullptr, 2 * pairs, 0, 2 * bits);
+        gp::Buf<gp::i64> first(d, 1);
+        const gp::i64 all_keys = 2 * pairs;
+        gp::to_device(d, first.get(), &all_keys, 1);
+        gp::launch(d, "sym_first_sentinel_kernel", gp::sym_first_sentinel_kernel, gp::stride_grid(d, 2 * pairs),
+                   gp::kThreads, 0, 2 * pairs, keys.get(), first.get());
+        GP_LAUNCH();
+        gp::i64 valid = 0;
+        gp::fetch(d, &valid, first.get(), 1);
+        gp::emit_symmetric(d, keys, alt, 2 * pairs, valid, n, bits, static_cast<gp::u64>((2 * pairs - valid) / 2),
+                           memory == GP_MEMORY_DEVICE, offsets_out, neighbors_out, neighbor_bytes, capacity, info,
+                           true);
     });
 }
 

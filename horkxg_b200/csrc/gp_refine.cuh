@@ -32,7 +32,26 @@ struct RefineCounters {
     i64 walked_degree;    // edges apply_cache_cut_kernel walked itself
     i64 hub_edges;        // edges of moving hubs walked by hub_apply_kernel
     i64 hub_chunks;       // their chunks
+    i64 filter_degree;    // edges of the LP proposers below the hub degree (profiling only)
 };
+
+// Profiling only: the edges the priority filter walks (proposers' rows below
+// the hub degree), into ctr->filter_degree.
+template <typename O>
+__global__ void filter_degree_kernel(const i32* __restrict__ list, const RefineCounters* ctr_in,
+                                     const O* __restrict__ off, RefineCounters* ctr) {
+    const i64 count = ctr_in->proposers;
+    i64 sum = 0;
+    for (i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<i64>(gridDim.x) * blockDim.x) {
+        const i32 v = list[i];
+        const i64 d = static_cast<i64>(off[v + 1]) - static_cast<i64>(off[v]);
+        if (d <= kHubDegree) sum += d;
+    }
+    sum = warp_sum(sum);
+    if ((threadIdx.x & 31) == 0 && sum)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->filter_degree), static_cast<unsigned long long>(sum));
+}
 
 // Per-vertex proposal record written by the LP pass: the priority filter
 // gathers one 16-byte record per neighbour instead of three arrays.
@@ -116,36 +135,78 @@ __device__ __forceinline__ void load_row(const C* row, int k, C (&vals)[32]) {
         if (p < k) vals[p] = row[p];
 }
 
-// incremental_build_affinity (src/refine_incremental.cuh:7-25), warp per
-// vertex.  Lanes holding the same part are grouped with __match_any_sync and
-// only the group leader adds to the warp's private row, so the row needs no
-// atomics.
+// incremental_build_affinity (src/refine_incremental.cuh:7-25).  A warp
+// takes four consecutive vertices: rows of at most 32 entries are walked by
+// 8 lanes each (up to four steps, all four rows at once), longer rows (up to
+// the hub degree) by the whole warp one after the other.  Lanes holding the
+// same part are grouped with __match_any_sync and only the group leader adds
+// to the row's private accumulator in shared memory, so no atomics are
+// needed; the four cache rows, consecutive in memory, are then stored by the
+// whole warp in one coalesced pass.  Hub rows are left to the chunked kernel
+// (zero_hub_rows_kernel clears them after this one).
 template <typename O, typename W, typename C>
 __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* __restrict__ off,
                                                                const i32* __restrict__ nbr, const W* __restrict__ ew,
                                                                const i32* __restrict__ labels, int k, C* cache) {
-    __shared__ u64 rows[kWarps][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ u64 rows[kWarps][4][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane >> 3, gl = lane & 7;
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
-    for (i64 v = static_cast<i64>(blockIdx.x) * kWarps + warp; v < n; v += warps_total) {
-        const i64 b = off[v], end = off[v + 1];
-        if (end - b > kHubDegree) continue;   // hub rows: chunked kernel
-        rows[warp][lane] = 0;
+    for (i64 q = static_cast<i64>(blockIdx.x) * kWarps + warp; q * 4 < n; q += warps_total) {
+        const i64 v = q * 4 + grp;
+        i64 b = 0, deg = 0;
+        if (v < n) {
+            b = static_cast<i64>(off[v]);
+            deg = static_cast<i64>(off[v + 1]) - b;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) rows[warp][grp][gl + 8 * j] = 0;
         __syncwarp();
-        for (i64 base = b; base < end; base += 32) {
-            const i64 e = base + lane;
+        const bool short_row = deg <= 32;
+        const unsigned steps = __reduce_max_sync(0xffffffffu, short_row ? static_cast<unsigned>((deg + 7) >> 3) : 0u);
+        for (unsigned r = 0; r < steps; ++r) {
+            const i64 e = static_cast<i64>(r) * 8 + gl;
             int p = -1;
             u64 w = 0;
-            if (e < end) {
-                const i32 u = nbr[e];
-                if (u != v) { p = labels[u]; w = static_cast<u64>(weight_at(ew, e)); }
+            if (short_row && e < deg) {
+                const i32 u = nbr[b + e];
+                if (u != v) { p = labels[u]; w = static_cast<u64>(weight_at(ew, b + e)); }
             }
-            const unsigned peers = __match_any_sync(0xffffffffu, p);
+            const unsigned peers = __match_any_sync(0xffffffffu, p < 0 ? -1 - grp : grp * 32 + p);
             const u64 sum = group_sum<C>(peers, w);
-            if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][p] += sum;
+            if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][grp][p] += sum;
             __syncwarp();
         }
-        if (lane < k) cache[v * k + lane] = static_cast<C>(rows[warp][lane]);
+        // rows of 33..kHubDegree entries, one at a time by the whole warp
+        unsigned longs = __ballot_sync(0xffffffffu, gl == 0 && !short_row && deg <= kHubDegree);
+        while (longs) {
+            const int src = __ffs(longs) - 1;
+            longs &= longs - 1;
+            const int g = src >> 3;
+            const i64 lb = __shfl_sync(0xffffffffu, b, src), ld = __shfl_sync(0xffffffffu, deg, src);
+            const i64 lv = q * 4 + g;
+            for (i64 base = 0; base < ld; base += 32) {
+                const i64 e = base + lane;
+                int p = -1;
+                u64 w = 0;
+                if (e < ld) {
+                    const i32 u = nbr[lb + e];
+                    if (u != lv) { p = labels[u]; w = static_cast<u64>(weight_at(ew, lb + e)); }
+                }
+                const unsigned peers = __match_any_sync(0xffffffffu, p);
+                const u64 sum = group_sum<C>(peers, w);
+                if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][g][p] += sum;
+                __syncwarp();
+            }
+        }
+        // the four rows are consecutive in the cache: entries [4qk, 4qk + 4k)
+        const i64 first = q * 4;
+        const int nrows = static_cast<int>(n - first < 4 ? n - first : 4);
+        const unsigned hub_rows = __ballot_sync(0xffffffffu, gl == 0 && deg > kHubDegree);
+        C* dst = cache + first * k;
+        for (int i = lane; i < nrows * k; i += 32) {
+            const int row = i / k;
+            if (!(hub_rows & (1u << (row * 8)))) dst[i] = static_cast<C>(rows[warp][row][i - row * k]);
+        }
         __syncwarp();
     }
 }

@@ -189,6 +189,9 @@ __device__ __forceinline__ void slot_candidate(i32 key, u64 conn, u32 v, i32 sou
                                                u64& current, u64& best, u64& tie) {
     if (key < 0) return;
     if (key == source) { current = conn; return; }
+    // a sum below the running best (or zero) never wins, whatever its tie
+    // key: skip the mover test and the tie hash for it
+    if (conn < best || conn == 0) return;
     if (p.filter && is_mover(key, p)) return;
     const u64 t = tie_key(v, key, p.tie_salt);
     if (better(conn, t, best, tie)) { best = conn; tie = t; }

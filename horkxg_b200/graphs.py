@@ -82,6 +82,28 @@ def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c:
     return _run(name, _lib().gp_gen_rmat, scale, edge_factor, a, b, c, seed)
 
 
+def rmat_device(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+                seed: int = 1, device: int = 0) -> tuple[Path, Path]:
+    """The files of rmat() made by the GPU generator (gp_generate_rmat),
+    which draws exactly the host generator's pairs and permutation: the same
+    bytes under the same cache name, in seconds instead of host minutes at
+    scale 26.  Needs a GPU."""
+    name = f"rmat_s{scale}_ef{edge_factor}_{a}_{b}_{c}_seed{seed}"
+    root = cache_dir() / name
+    root.mkdir(parents=True, exist_ok=True)
+    indptr, indices = root / "indptr.bin", root / "indices.bin"
+    if indptr.exists() and indices.exists():
+        return indptr, indices
+    import horkxg_b200 as hb
+    with hb.Context(device) as ctx:
+        off, nbr, _ = ctx.generate_rmat(scale, edge_factor, a, b, c, seed)
+    for path, arr in ((indptr, off), (indices, nbr)):
+        tmp = path.with_suffix(".tmp")
+        arr.tofile(tmp)
+        tmp.rename(path)
+    return indptr, indices
+
+
 def rgg(n: int, mean_degree: float = 10.0, seed: int = 7) -> tuple[Path, Path]:
     radius = math.sqrt(mean_degree / (math.pi * n))
     return _run(f"rgg_n{n}_deg{mean_degree}_seed{seed}", _lib().gp_gen_rgg, n, radius, seed)
@@ -204,7 +226,7 @@ def by_name(name: str) -> tuple[Path, Path]:
         "rmat20": lambda: rmat(20),
         "rmat22": lambda: rmat(22),
         "rmat24": lambda: rmat(24),
-        "rmat26": lambda: rmat(26),
+        "rmat26": lambda: rmat_device(26),
         "rgg_20k": lambda: rgg(20000),
         "cycle_hub_4096": cycle_hub,
     }

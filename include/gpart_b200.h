@@ -244,6 +244,41 @@ typedef struct gp_analysis {
 gp_status gp_analyze(gp_ctx* ctx, const gp_graph* graph, const int32_t* labels, int parts, gp_part_stats* per_part,
                      gp_analysis* summary);
 
+/* Symmetrise and deduplicate a CSR (replaces graph_untils/csr_symmetrize.cpp:
+ * 277-538, the reference's preprocessing of directed or asymmetric inputs):
+ * every entry (v, u) with u != v stands for the undirected edge {u, v}; self
+ * loops are dropped; the output holds both directions of every distinct edge,
+ * rows ascending by neighbour -- the same offsets and indices the reference
+ * writes.  Edge and vertex weights of the input are ignored (the output is
+ * unweighted, as the reference's).  offsets_out: n + 1 int64; neighbors_out:
+ * `capacity` entries of neighbor_bytes (4 = int32, 8 = int64 as in the
+ * reference's files); both in host memory when graph->memory is HOST, else
+ * device memory.  At most 2 * m entries are needed; when `capacity` is
+ * smaller than the output, nothing is written, info still reports the sizes
+ * and GP_EINVAL is returned. */
+typedef struct gp_symmetrize_info {
+    int64_t self_loops_removed;
+    int64_t unique_undirected_edges;
+    int64_t output_directed_edges;   /* entries of the symmetric CSR */
+} gp_symmetrize_info;
+
+gp_status gp_symmetrize(gp_ctx* ctx, const gp_graph* graph, int64_t* offsets_out, void* neighbors_out,
+                        int32_t neighbor_bytes, int64_t capacity, gp_symmetrize_info* info);
+
+/* R-MAT graph generated on the GPU: 2^scale vertices, edge_factor * 2^scale
+ * pairs with quadrant probabilities (a, b, c, 1 - a - b - c), vertex ids
+ * relabelled by a seeded permutation, then symmetrised like gp_symmetrize.
+ * The pairs and the permutation are drawn exactly as the package's host
+ * generator draws them (horkxg_b200/graphs.py rmat(), the graphs both bench
+ * arms read), so the CSR is identical to that generator's files.  No
+ * counterpart in the reference, whose RMAT inputs come from its tools'
+ * external files; this makes the largest configured inputs (RMAT-26) without
+ * the host.  Output as in gp_symmetrize, in host or device memory per
+ * `memory` (GP_MEMORY_HOST / GP_MEMORY_DEVICE). */
+gp_status gp_generate_rmat(gp_ctx* ctx, int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                           int32_t memory, int64_t* offsets_out, void* neighbors_out, int32_t neighbor_bytes,
+                           int64_t capacity, gp_symmetrize_info* info);
+
 /* Kernel launches issued by this context so far (all of them are the
  * library's own sm_100a kernels). */
 uint64_t gp_launch_count(const gp_ctx* ctx);
@@ -264,6 +299,13 @@ gp_status gp_ctx_set_device_share(gp_ctx* ctx, int share);
  * instead of a cooperative grid; both compute the same values.  enable = 0 keeps the
  * grid kernel for every graph (default 1). */
 gp_status gp_ctx_set_small_diffusion(gp_ctx* ctx, int enable);
+
+/* Hubs (vertices of more than 2048 edges) aggregate their neighbours'
+ * clusters in hash tables.  on_chip = 1 (default) keeps the table of every hub
+ * of up to about 9,400 edges in one CTA's shared memory, on levels whose
+ * total edge weight fits 32 bits; 0 keeps every table in global memory.  Both
+ * give the same hierarchy. */
+gp_status gp_ctx_set_hub_tables(gp_ctx* ctx, int on_chip);
 
 /* Spectral initial partition that allocates no device memory.
  *

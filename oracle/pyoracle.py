@@ -220,3 +220,24 @@ def hierarchy_file_digests(levels, maps):
         blob = b"".join(p.tobytes() for p in parts)
         out.append({"n": int(g.n), "m": int(len(g.nbr)), "sha256": hashlib.sha256(blob).hexdigest()})
     return out
+
+
+def symmetrize(offsets, indices):
+    """The reference's CSR symmetriser (graph_untils/csr_symmetrize.cpp:
+    277-538) restated with numpy: every entry (v, u), u != v, is the
+    undirected edge {min, max} (:298-311); the distinct edges (:346-378) are
+    written in both directions sorted by (source, neighbour) (:461-537);
+    self loops are counted and dropped.  Returns (int64 offsets, int64
+    indices, self loops)."""
+    off = np.asarray(offsets, np.int64)
+    idx = np.asarray(indices, np.int64)
+    n = len(off) - 1
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    keep = src != idx
+    lo, hi = np.minimum(src[keep], idx[keep]), np.maximum(src[keep], idx[keep])
+    edges = np.unique(lo * n + hi)
+    u, v = edges // n, edges % n
+    both = np.sort(np.concatenate([u * n + v, v * n + u]))
+    out_off = np.zeros(n + 1, np.int64)
+    out_off[1:] = np.cumsum(np.bincount(both // n, minlength=n))
+    return out_off, both % n, int((~keep).sum())

@@ -24,9 +24,11 @@ def reference_report(indptr, indices, labels, parts, tmp_path):
     out = subprocess.run([str(ANALYZER), "--partition", str(txt), "--indptr", str(indptr), "--indices",
                           str(indices), "--parts", str(parts), "--detail"], capture_output=True, text=True,
                          check=True).stdout
-    counts = out.split("Per-Part Metrics: Counts")[1].split("=====")[1]
-    rows = [list(map(int, line.split())) for line in counts.strip().splitlines()[1:]]
-    quality = out.split("Partition Quality")[1].splitlines()[3].split()
+    def section(title):   # the lines between a section's title line and the next blank line
+        lines = out.split(f"=========== {title} ===========\n", 1)[1].splitlines()
+        return lines[:lines.index("")] if "" in lines else lines
+    rows = [list(map(int, line.split())) for line in section("Per-Part Metrics: Counts")[1:]]
+    quality = section("Partition Quality")[1].split()
     return np.array(rows, np.int64), {"edge_cut": int(quality[2]), "vertex_imb": float(quality[4]),
                                       "edge_imb": float(quality[5]), "avg_local_cut": float(quality[6]),
                                       "max_local_cut": int(quality[7])}

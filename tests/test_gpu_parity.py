@@ -442,7 +442,7 @@ def test_verify_driver_prints_layer_checks(ctx, tmp_path):
     assert r.returncode == 0, r.stderr
     lines = re.findall(r"^ml_layer_verify level=(\d+) map=ok weights=ok csr=ok projection_cut=ok$", r.stdout, re.M)
     _, _, g = file_graph("grid2d_256")
-    levels = ctx.partition(g, parts=4).levels      # the hierarchy does not depend on the refinement
+    levels = ctx.partition(g, parts=4)[1].levels   # the hierarchy does not depend on the refinement
     assert [int(x) for x in lines] == list(range(levels - 1))
 
 

@@ -238,3 +238,29 @@ def test_oracle_partition_from_its_own_initial_partition():
     levels, _ = O.coarsen(g, 8)
     init = O.initial_partition(levels[-1], 8)
     assert np.array_equal(O.partition_from(g, 8, init)[0], O.partition(g, 8)[0])
+
+
+def test_oracle_symmetrize_matches_reference_tool(tmp_path):
+    # the numpy restatement against the reference's own CPU tool, built from
+    # its source by oracle/Makefile (graph_untils/csr_symmetrize.cpp)
+    import subprocess
+    from pathlib import Path
+    tool = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "csr_symmetrize"
+    if not tool.exists():
+        pytest.skip("the reference tool is built only where its sources are present")
+    rng = np.random.default_rng(11)
+    n = 700
+    deg = rng.integers(0, 15, n)
+    off = np.zeros(n + 1, np.int64)
+    off[1:] = np.cumsum(deg)
+    idx = rng.integers(0, n, int(off[-1])).astype(np.int64)
+    idx[::11] = np.repeat(np.arange(n), deg)[::11]
+    off.tofile(tmp_path / "p.bin")
+    idx.tofile(tmp_path / "i.bin")
+    out = subprocess.run([str(tool), "--indptr", str(tmp_path / "p.bin"), "--indices", str(tmp_path / "i.bin"),
+                          "--output-dir", str(tmp_path / "o"), "--output-name", "g"], capture_output=True,
+                         text=True, check=True).stdout
+    eo, ei, loops = O.symmetrize(off, idx)
+    assert np.array_equal(np.fromfile(tmp_path / "o" / "g_indptr.bin", np.int64), eo)
+    assert np.array_equal(np.fromfile(tmp_path / "o" / "g_indices.bin", np.int64), ei)
+    assert f"self_loops_removed: {loops}" in out
