@@ -192,7 +192,7 @@ struct HubPartial { u64 current, best, tie; };
 
 // ---------------------------------------------------------------------------
 // SCLP affinity of hubs whose table fits in one CTA's shared memory (up to
-// ~9.4K edges): one CTA per hub does the inserts, the candidate scan and the
+// ~22K edges): one CTA per hub does the inserts, the candidate scan and the
 // decode in one launch, so these tables never reach global memory and need
 // neither a clearing memset nor a separate candidate pass.  8-byte slots
 // (cluster + 1, 32-bit sum) claimed by one 64-bit CAS, as HubSlot32: used on
@@ -200,9 +200,12 @@ struct HubPartial { u64 current, best, tie; };
 // global tables: one CTA walking 10^4-10^5 edges would be a long chain of
 // dependent loads, where the chunks spread a hub over many CTAs.
 // ---------------------------------------------------------------------------
+// Two shapes: hubs whose table fits 96 KB run 512 threads, two CTAs per SM;
+// hubs up to the largest table one CTA can hold (~227 KB) run 1024 threads,
+// one CTA per SM.
+constexpr int kHubSmemSlots = 12288;        // 96 KB
 constexpr int kHubSmemThreads = 512;
-constexpr int kHubSmemWarps = kHubSmemThreads / 32;
-constexpr int kHubSmemSlots = 12288;        // 96 KB, two CTAs per SM
+constexpr int kHubMidThreads = 1024;        // its table: what the device's per-CTA limit leaves (hub_mid_slots)
 
 // Table slots for a hub of `degree` edges: at least 1.3x the degree (a hub
 // has at most `degree` distinct neighbour clusters), whole 32-slot lines.
@@ -211,12 +214,14 @@ __host__ __device__ inline i64 hub_smem_slots(i64 degree) {
     return (want + 31) / 32 * 32;
 }
 
-template <typename O, typename W>
-__global__ void __launch_bounds__(kHubSmemThreads) hub_smem_kernel(
+template <int THREADS, typename O, typename W>
+__global__ void __launch_bounds__(THREADS) hub_smem_kernel(
     const i32* __restrict__ hub_ids, const O* __restrict__ off, const i32* __restrict__ nbr,
     const W* __restrict__ ew, const W* __restrict__ vw, const i32* __restrict__ clusters,
     const u64* __restrict__ cw, RoundParams p, SclpOut out) {
-    extern __shared__ unsigned long long table[];   // kHubSmemSlots at most
+    constexpr int kHubSmemWarps = THREADS / 32;
+    constexpr int kHubSmemThreads = THREADS;
+    extern __shared__ unsigned long long table[];   // hub_smem_slots(degree) entries
     __shared__ u64 red[3][kHubSmemWarps];
     const i32 v = hub_ids[blockIdx.x];
     const i32 source = clusters[v];

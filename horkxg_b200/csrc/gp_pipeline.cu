@@ -85,11 +85,14 @@ struct DGraph {
         Buf<Chunk> chunk;
         Buf<i64> chunk_begin;   // per hub, count + 1 entries
         // SCLP affinity split (hub_split): the hubs whose table fits one
-        // CTA's shared memory (chip_ids), and the hubs that keep global
-        // tables, with their own chunk list (Chunk::hub indexes global_list)
+        // CTA's shared memory (chip_ids: the 96 KB shape first, chip_count
+        // of them, then mid_count hubs of the 227 KB shape), and the hubs
+        // that keep global tables, with their own chunk list (Chunk::hub
+        // indexes global_list)
         bool split_built = false;
         Buf<i32> chip_ids;
-        i64 chip_count = 0;
+        i64 chip_count = 0, mid_count = 0;
+        i64 mid_slots = 0;   // table slots of the 1024-thread shape on this device
         i64 global_count = 0, global_chunks = 0;
         Buf<i32> global_list;
         Buf<Chunk> global_chunk;
@@ -155,12 +158,24 @@ const typename DGraph<T>::Hubs& hub_split(Device& d, const DGraph<T>& g) {
         to_host(d, ids.data(), hubs.list.get(), ids.size());
         d.sync();
     }
-    std::vector<i32> chip, glob;
+    // the largest table one CTA of the 1024-thread shape can hold: the
+    // device's opt-in shared memory per block less the kernel's static part,
+    // whole 32-slot lines
+    int optin = 0;
+    GP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device));
+    cudaFuncAttributes fa{};
+    GP_CUDA(cudaFuncGetAttributes(&fa, hub_smem_kernel<kHubMidThreads, O, typename T::W>));
+    h.mid_slots = std::max<i64>(0, (static_cast<i64>(optin) - static_cast<i64>(fa.sharedSizeBytes)) / 8 / 32 * 32);
+    std::vector<i32> chip, mid, glob;
     std::vector<Chunk> chunks;
     for (i64 i = 0; i < hubs.count; ++i) {
         const i64 begin = ext[2 * i], degree = ext[2 * i + 1];
         if (hub_smem_slots(degree) <= kHubSmemSlots) {
             chip.push_back(ids[i]);
+            continue;
+        }
+        if (hub_smem_slots(degree) <= h.mid_slots) {
+            mid.push_back(ids[i]);
             continue;
         }
         const i32 gi = static_cast<i32>(glob.size());
@@ -169,6 +184,8 @@ const typename DGraph<T>::Hubs& hub_split(Device& d, const DGraph<T>& g) {
             chunks.push_back({ids[i], gi, e, std::min(e + kChunkEdges, begin + degree)});
     }
     h.chip_count = static_cast<i64>(chip.size());
+    h.mid_count = static_cast<i64>(mid.size());
+    chip.insert(chip.end(), mid.begin(), mid.end());
     if (!chip.empty()) {
         h.chip_ids = Buf<i32>(d, chip.size());
         to_device(d, h.chip_ids.get(), chip.data(), chip.size());
@@ -498,10 +515,17 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
                                                 chip_edges * (4 + 4 + (ew ? sizeof(W) : 0)));
             if (hubs.chip_count) {
                 const size_t smem = static_cast<size_t>(kHubSmemSlots) * sizeof(unsigned long long);
-                GP_CUDA(cudaFuncSetAttribute(hub_smem_kernel<O, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem)));
-                launch(d, "hub_smem_kernel", hub_smem_kernel<O, W>, static_cast<int>(hubs.chip_count),
-                       kHubSmemThreads, smem, hubs.chip_ids.get(), off, nbr, ew, vw, clusters, cw, p, so);
+                auto k = hub_smem_kernel<kHubSmemThreads, O, W>;
+                GP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+                launch(d, "hub_smem_kernel", k, static_cast<int>(hubs.chip_count), kHubSmemThreads, smem,
+                       hubs.chip_ids.get(), off, nbr, ew, vw, clusters, cw, p, so);
+            }
+            if (hubs.mid_count) {
+                const size_t smem = static_cast<size_t>(hubs.mid_slots) * sizeof(unsigned long long);
+                auto k = hub_smem_kernel<kHubMidThreads, O, W>;
+                GP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+                launch(d, "hub_smem_kernel", k, static_cast<int>(hubs.mid_count), kHubMidThreads, smem,
+                       hubs.chip_ids.get() + hubs.chip_count, off, nbr, ew, vw, clusters, cw, p, so);
             }
         }
         if (cnt[5] && gcount) {
