@@ -520,15 +520,19 @@ __global__ void __launch_bounds__(kThreads) giant_place_kernel(const SegChunk* _
 
 // Classifies coarse rows by their number of scattered entries: counts[c]
 // receives the rows of class c, counts[kRowClasses + c] their entries.
-__global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, u64* keys, i32* vals, u64* counts) {
+// `bitmap_from`: rows longer than this (up to kGiantSeg) take the bitmap
+// ranking of class 5 whatever their class by length, since on levels with
+// few coarse vertices a bitmap over the id range costs less than sorting.
+__global__ void row_class_kernel(i64 rows, const i64* temp_off, i64 smem_cap, i64 bitmap_from, u64* keys, i32* vals,
+                                 u64* counts) {
     __shared__ unsigned long long local[2 * kRowClasses];
     if (threadIdx.x < 2 * kRowClasses) local[threadIdx.x] = 0;
     __syncthreads();
     const i64 c = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c < rows) {
         const i64 l = temp_off[c + 1] - temp_off[c];
-        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kWarpSegCap ? 2 : l <= kMidSegCap ? 3 : l <= smem_cap ? 4
-                    : l <= kGiantSeg ? 5 : 6;
+        const int k = l == 0 ? 0 : l <= 32 ? 1 : l <= kWarpSegCap ? 2 : (l > bitmap_from && l <= kGiantSeg) ? 5
+                    : l <= kMidSegCap ? 3 : l <= smem_cap ? 4 : l <= kGiantSeg ? 5 : 6;
         keys[c] = static_cast<u64>(k);
         vals[c] = static_cast<i32>(c);
         atomicAdd(&local[k], 1ull);

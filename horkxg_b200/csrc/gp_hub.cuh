@@ -200,9 +200,11 @@ struct HubPartial { u64 current, best, tie; };
 // global tables: one CTA walking 10^4-10^5 edges would be a long chain of
 // dependent loads, where the chunks spread a hub over many CTAs.
 // ---------------------------------------------------------------------------
-// Two shapes: hubs whose table fits 96 KB run 512 threads, two CTAs per SM;
-// hubs up to the largest table one CTA can hold (~227 KB) run 1024 threads,
-// one CTA per SM.
+// Three shapes: hubs whose table fits 42 KB (up to ~4.1K edges, most hubs of
+// an RMAT level) run 512 threads with four CTAs per SM; up to 96 KB, 512
+// threads with two CTAs per SM; up to the largest table one CTA can hold
+// (~227 KB), 1024 threads with one CTA per SM.
+constexpr int kHubSmallSlots = 5376;        // 42 KB
 constexpr int kHubSmemSlots = 12288;        // 96 KB
 constexpr int kHubSmemThreads = 512;
 constexpr int kHubMidThreads = 1024;        // its table: what the device's per-CTA limit leaves (hub_mid_slots)

@@ -85,13 +85,13 @@ struct DGraph {
         Buf<Chunk> chunk;
         Buf<i64> chunk_begin;   // per hub, count + 1 entries
         // SCLP affinity split (hub_split): the hubs whose table fits one
-        // CTA's shared memory (chip_ids: the 96 KB shape first, chip_count
-        // of them, then mid_count hubs of the 227 KB shape), and the hubs
-        // that keep global tables, with their own chunk list (Chunk::hub
-        // indexes global_list)
+        // CTA's shared memory (chip_ids: small_count hubs of the 42 KB shape,
+        // then chip_count of the 96 KB shape, then mid_count of the 227 KB
+        // shape), and the hubs that keep global tables, with their own chunk
+        // list (Chunk::hub indexes global_list)
         bool split_built = false;
         Buf<i32> chip_ids;
-        i64 chip_count = 0, mid_count = 0;
+        i64 small_count = 0, chip_count = 0, mid_count = 0;
         i64 mid_slots = 0;   // table slots of the 1024-thread shape on this device
         i64 global_count = 0, global_chunks = 0;
         Buf<i32> global_list;
@@ -166,10 +166,14 @@ const typename DGraph<T>::Hubs& hub_split(Device& d, const DGraph<T>& g) {
     cudaFuncAttributes fa{};
     GP_CUDA(cudaFuncGetAttributes(&fa, hub_smem_kernel<kHubMidThreads, O, typename T::W>));
     h.mid_slots = std::max<i64>(0, (static_cast<i64>(optin) - static_cast<i64>(fa.sharedSizeBytes)) / 8 / 32 * 32);
-    std::vector<i32> chip, mid, glob;
+    std::vector<i32> small, chip, mid, glob;
     std::vector<Chunk> chunks;
     for (i64 i = 0; i < hubs.count; ++i) {
         const i64 begin = ext[2 * i], degree = ext[2 * i + 1];
+        if (hub_smem_slots(degree) <= kHubSmallSlots) {
+            small.push_back(ids[i]);
+            continue;
+        }
         if (hub_smem_slots(degree) <= kHubSmemSlots) {
             chip.push_back(ids[i]);
             continue;
@@ -183,12 +187,14 @@ const typename DGraph<T>::Hubs& hub_split(Device& d, const DGraph<T>& g) {
         for (i64 e = begin; e < begin + degree; e += kChunkEdges)
             chunks.push_back({ids[i], gi, e, std::min(e + kChunkEdges, begin + degree)});
     }
+    h.small_count = static_cast<i64>(small.size());
     h.chip_count = static_cast<i64>(chip.size());
     h.mid_count = static_cast<i64>(mid.size());
-    chip.insert(chip.end(), mid.begin(), mid.end());
-    if (!chip.empty()) {
-        h.chip_ids = Buf<i32>(d, chip.size());
-        to_device(d, h.chip_ids.get(), chip.data(), chip.size());
+    small.insert(small.end(), chip.begin(), chip.end());
+    small.insert(small.end(), mid.begin(), mid.end());
+    if (!small.empty()) {
+        h.chip_ids = Buf<i32>(d, small.size());
+        to_device(d, h.chip_ids.get(), small.data(), small.size());
     }
     h.global_count = static_cast<i64>(glob.size());
     h.global_chunks = static_cast<i64>(chunks.size());
@@ -513,19 +519,27 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
             const double chip_hubs = static_cast<double>(work[5][0] - gwork[0]);
             d.prof_bytes("hub_smem_kernel", chip_hubs * (2 * sizeof(O) + 4 + 4 + 8 + 4 + 8) +
                                                 chip_edges * (4 + 4 + (ew ? sizeof(W) : 0)));
-            if (hubs.chip_count) {
-                const size_t smem = static_cast<size_t>(kHubSmemSlots) * sizeof(unsigned long long);
-                auto k = hub_smem_kernel<kHubSmemThreads, O, W>;
-                GP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-                launch(d, "hub_smem_kernel", k, static_cast<int>(hubs.chip_count), kHubSmemThreads, smem,
-                       hubs.chip_ids.get(), off, nbr, ew, vw, clusters, cw, p, so);
-            }
+            // the attribute is the largest size any launch of the kernel
+            // uses (server slots share it across threads): never lowered
+            const size_t smem512 = static_cast<size_t>(kHubSmemSlots) * sizeof(unsigned long long);
+            auto k512 = hub_smem_kernel<kHubSmemThreads, O, W>;
+            if (hubs.small_count || hubs.chip_count)
+                GP_CUDA(cudaFuncSetAttribute(k512, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem512)));
+            if (hubs.small_count)
+                launch(d, "hub_smem_kernel", k512, static_cast<int>(hubs.small_count), kHubSmemThreads,
+                       static_cast<size_t>(kHubSmallSlots) * sizeof(unsigned long long), hubs.chip_ids.get(), off,
+                       nbr, ew, vw, clusters, cw, p, so);
+            if (hubs.chip_count)
+                launch(d, "hub_smem_kernel", k512, static_cast<int>(hubs.chip_count), kHubSmemThreads, smem512,
+                       hubs.chip_ids.get() + hubs.small_count, off, nbr, ew, vw, clusters, cw, p, so);
             if (hubs.mid_count) {
                 const size_t smem = static_cast<size_t>(hubs.mid_slots) * sizeof(unsigned long long);
                 auto k = hub_smem_kernel<kHubMidThreads, O, W>;
                 GP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
                 launch(d, "hub_smem_kernel", k, static_cast<int>(hubs.mid_count), kHubMidThreads, smem,
-                       hubs.chip_ids.get() + hubs.chip_count, off, nbr, ew, vw, clusters, cw, p, so);
+                       hubs.chip_ids.get() + hubs.small_count + hubs.chip_count, off, nbr, ew, vw, clusters, cw, p,
+                       so);
             }
         }
         if (cnt[5] && gcount) {
@@ -722,8 +736,13 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     Buf<i32> rl(d, static_cast<size_t>(coarse_n)), rl_alt(d, static_cast<size_t>(coarse_n));
     Buf<u64> rc(d, 2 * kRowClasses);
     rc.zero(d);
+    // A row is ranked by the bitmap of segment_bitmap_kernel instead of a
+    // shared-memory sort once it is longer than coarse_n / 64: the bitmap
+    // costs about coarse_n / 32 words per window plus two passes over the row,
+    // the sort three passes with barriers; both give the same row.
+    const i64 bitmap_from = std::max<i64>(kWarpSegCap, coarse_n / 64);
     launch(d, "row_class_kernel", row_class_kernel, blocks_for(coarse_n, kThreads), kThreads, 0, coarse_n,
-           temp_off.get(), static_cast<i64>(seg_smem_capacity<W>()), rk.get(), rl.get(), rc.get());
+           temp_off.get(), static_cast<i64>(seg_smem_capacity<W>()), bitmap_from, rk.get(), rl.get(), rc.get());
     GP_LAUNCH();
     radix_sort<u64, i32>(d, rk.get(), rl.get(), rk_alt.get(), rl_alt.get(), coarse_n, 0, 8);
     u64 rcnt[2 * kRowClasses];
