@@ -98,7 +98,7 @@ EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_erro
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
            "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_set_hub_tables", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
-           "gp_initial_partition_static", "gp_initial_partition_trace", "gp_analyze", "gp_symmetrize", "gp_generate_rmat", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim",
+           "gp_initial_partition_static", "gp_initial_partition_trace", "gp_analyze", "gp_symmetrize", "gp_generate_rmat", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim", "gp_ctx_allocator_stats",
            "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
            "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
 
@@ -154,6 +154,7 @@ def lib() -> ctypes.CDLL:
         L.gp_partition_range.argtypes = [vp, P(GraphDesc), i64, i64, P(Options), vp, P(Report)]
         L.gp_ctx_memory.argtypes = [vp, P(u64), P(u64), P(u64), i32]
         L.gp_ctx_trim.argtypes = [vp]
+        L.gp_ctx_allocator_stats.argtypes = [vp, P(u64), P(u64), P(u64), P(dbl)]
         L.gp_footprint_bytes.argtypes = [i64, i64, i32, i32, i32]
         L.gp_footprint_bytes.restype = u64
         L.gp_server_create.argtypes = [i32, i32, u64, P(vp)]
@@ -463,6 +464,14 @@ class Context:
         self._check(lib().gp_ctx_memory(self._h, ctypes.byref(live), ctypes.byref(cached), ctypes.byref(peak),
                                         int(reset_peak)))
         return {"live": live.value, "cached": cached.value, "peak": peak.value}
+
+    def allocator_stats(self) -> dict:
+        """Caching-allocator counters: requests, driver allocations, cached
+        blocks freed to make room, host milliseconds in the allocator."""
+        r, a, f, ms = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
+        self._check(lib().gp_ctx_allocator_stats(self._h, ctypes.byref(r), ctypes.byref(a), ctypes.byref(f),
+                                                 ctypes.byref(ms)))
+        return {"requests": r.value, "driver_allocs": a.value, "cache_frees": f.value, "host_ms": ms.value}
 
     def trim(self):
         self._check(lib().gp_ctx_trim(self._h))

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cstring>
 #include <cstdio>
+#include <iterator>
 #include <map>
 #include <unordered_map>
 #include <stdexcept>
@@ -96,10 +97,13 @@ struct Device {
     void* pinned = nullptr;     // small pinned host staging area
     static constexpr size_t kPinnedBytes = 1 << 16;
 
+    cudaError_t driver_alloc(void** p, size_t bytes) { return cudaMalloc(p, bytes); }
+    void driver_free(void* p) { cudaFree(p); }
+
     std::map<size_t, std::vector<void*>> free_blocks;
     std::unordered_map<void*, size_t> live;
     size_t cached_bytes = 0, live_bytes = 0, peak_bytes = 0;
-    u64 alloc_calls = 0, driver_allocs = 0;
+    u64 alloc_calls = 0, driver_allocs = 0, cache_frees = 0;
     double alloc_ms = 0.0;   // host time spent inside the allocator
 
     static size_t size_class(size_t bytes) {
@@ -113,9 +117,39 @@ struct Device {
         if (cached_bytes == 0) return;
         cudaStreamSynchronize(stream);
         for (auto& kv : free_blocks)
-            for (void* p : kv.second) cudaFree(p);
+            for (void* p : kv.second) driver_free(p);
         free_blocks.clear();
         cached_bytes = 0;
+    }
+    // Makes room for a `bytes` allocation that the driver refused: frees the
+    // smallest cached block at least that large, or, without one, cached
+    // blocks largest first until `bytes` are returned.  The rest of the cache
+    // stays for the blocks that will be asked for again (a full flush made
+    // every partition of the largest graphs re-allocate most of its blocks).
+    void release_cached(size_t bytes) {
+        if (cached_bytes == 0) return;
+        cudaStreamSynchronize(stream);
+        for (auto fit = free_blocks.lower_bound(bytes); fit != free_blocks.end(); ++fit) {
+            if (fit->second.empty()) continue;
+            driver_free(fit->second.back());
+            fit->second.pop_back();
+            cached_bytes -= fit->first;
+            ++cache_frees;
+            if (fit->second.empty()) free_blocks.erase(fit);
+            return;
+        }
+        size_t freed = 0;
+        while (freed < bytes && !free_blocks.empty()) {
+            auto it = std::prev(free_blocks.end());
+            while (!it->second.empty() && freed < bytes) {
+                driver_free(it->second.back());
+                it->second.pop_back();
+                freed += it->first;
+                cached_bytes -= it->first;
+                ++cache_frees;
+            }
+            if (it->second.empty()) free_blocks.erase(it);
+        }
     }
     void* alloc(size_t bytes) {
         if (bytes == 0) return nullptr;
@@ -128,11 +162,16 @@ struct Device {
             it->second.pop_back();
             cached_bytes -= c;
         } else {
-            cudaError_t e = cudaMalloc(&p, c);
+            cudaError_t e = driver_alloc(&p, c);
+            if (e != cudaSuccess) {   // release part of the cache, then all of it
+                cudaGetLastError();
+                release_cached(c);
+                e = driver_alloc(&p, c);
+            }
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 release_cached();
-                e = cudaMalloc(&p, c);
+                e = driver_alloc(&p, c);
             }
             if (e != cudaSuccess) {
                 cudaGetLastError();

@@ -321,6 +321,36 @@ __global__ void __launch_bounds__(kThreads) segment_smem_kernel(i64 rows, const 
     if (threadIdx.x == 0) row_len[c] = u;
 }
 
+// Rows of the bitmap class on levels whose coarse id range spans more than
+// kSortWindows bitmap windows: the bitmap kernel rescans the row once per
+// window, so here one block sorts the row where it lies instead -- LSD radix
+// passes ping-ponging between the row's segment and its alternate buffer
+// (global memory, mostly L2-resident for rows of at most kGiantSeg entries),
+// then its runs reduced into the alternate buffer.  Same output as
+// segment_bitmap_kernel: rows sorted by target, duplicates summed, internal
+// edges (the sentinel, which sorts last) dropped.
+constexpr i64 kSortWindows = 4;
+
+template <typename W>
+__global__ void __launch_bounds__(kThreads) segment_sort_kernel(i64 rows, const i32* __restrict__ list,
+                                                                const i64* __restrict__ temp_off,
+                                                                const i64* __restrict__ alt_off, u32 sentinel,
+                                                                int key_bits, u32* tgt, W* wt, u32* alt_k, W* alt_w,
+                                                                i64* row_len) {
+    __shared__ RankShared rank_sh;
+    __shared__ RunShared<W> run_sh;
+    const i64 r = blockIdx.x;
+    if (r >= rows) return;
+    const i32 c = list[r];
+    const i64 s = temp_off[c];
+    const i64 len = temp_off[c + 1] - s;
+    u32* k_alt = alt_k + alt_off[r];
+    W* w_alt = alt_w + alt_off[r];
+    block_radix_sort_segment(tgt + s, wt + s, k_alt, w_alt, len, 0, key_bits, rank_sh);
+    const i64 u = block_reduce_runs(tgt + s, wt + s, len, sentinel, k_alt, w_alt, run_sh);
+    if (threadIdx.x == 0) row_len[c] = u;
+}
+
 // Rows above seg_smem_capacity entries: block per row, no sort.  The row's
 // distinct targets are marked in a shared-memory bitmap over a window of the
 // coarse id range; a target's output position is then the number of marked

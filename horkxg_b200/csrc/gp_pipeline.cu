@@ -755,7 +755,8 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
     d.prof_bytes("segment_warp_kernel", seg_bytes(1));
     d.prof_bytes("segment_warp_radix_kernel", seg_bytes(2));
     d.prof_bytes("segment_smem_kernel", seg_bytes(3) + seg_bytes(4));
-    d.prof_bytes("segment_bitmap_kernel", seg_bytes(5));
+    const bool sort_big = (coarse_n + kBitmapWindow - 1) / kBitmapWindow > kSortWindows;
+    d.prof_bytes(sort_big ? "segment_sort_kernel" : "segment_bitmap_kernel", seg_bytes(5));
     d.prof_bytes("giant_place_kernel", seg_bytes(6));
     Buf<i64> row_len(d, static_cast<size_t>(coarse_n) + 1);
     row_len.zero(d);
@@ -800,7 +801,12 @@ void contract(Device& d, const DGraph<T>& g, const i32* map, i64 coarse_n, Buf<t
         ak = Buf<u32>(d, static_cast<size_t>(alt_total));
         aw = Buf<W>(d, static_cast<size_t>(alt_total));
     }
-    if (rcnt[5]) {
+    if (rcnt[5] && sort_big) {
+        launch(d, "segment_sort_kernel", segment_sort_kernel<W>, static_cast<int>(rcnt[5]), kThreads, 0,
+               static_cast<i64>(rcnt[5]), rl.get() + c3, temp_off.get(), alt_off.get(), sentinel, key_bits, tgt.get(),
+               wt.get(), ak.get(), aw.get(), row_len.get());
+        GP_LAUNCH();
+    } else if (rcnt[5]) {
         const size_t smem = (static_cast<size_t>(kBitmapWords) + kBitmapGroups) * sizeof(u32);
         GP_CUDA(cudaFuncSetAttribute(segment_bitmap_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
@@ -2298,7 +2304,7 @@ void gp_ctx_destroy(gp_ctx* ctx) {
     cudaSetDevice(d.device);
     if (d.stream) cudaStreamSynchronize(d.stream);
     d.release_cached();
-    for (auto& kv : d.live) cudaFree(kv.first);
+    for (auto& kv : d.live) d.driver_free(kv.first);
     d.live.clear();
     for (auto e : d.event_pool) cudaEventDestroy(e);
     if (d.sync_event) cudaEventDestroy(d.sync_event);
@@ -2494,6 +2500,16 @@ gp_status gp_ctx_memory(gp_ctx* ctx, uint64_t* live, uint64_t* cached, uint64_t*
     if (cached) *cached = d.cached_bytes;
     if (peak) *peak = d.peak_bytes;
     if (reset_peak) d.peak_bytes = d.live_bytes;
+    return GP_OK;
+}
+
+gp_status gp_ctx_allocator_stats(gp_ctx* ctx, uint64_t* requests, uint64_t* driver_allocs, uint64_t* cache_frees,
+                                 double* host_ms) {
+    if (!ctx) return GP_EINVAL;
+    if (requests) *requests = ctx->dev.alloc_calls;
+    if (driver_allocs) *driver_allocs = ctx->dev.driver_allocs;
+    if (cache_frees) *cache_frees = ctx->dev.cache_frees;
+    if (host_ms) *host_ms = ctx->dev.alloc_ms;
     return GP_OK;
 }
 

@@ -145,6 +145,13 @@ gp_status gp_partition_range(gp_ctx* ctx, const gp_graph* packed, int64_t vertex
  * value).  gp_ctx_trim returns the cached blocks to the driver. */
 gp_status gp_ctx_memory(gp_ctx* ctx, uint64_t* live, uint64_t* cached, uint64_t* peak, int reset_peak);
 gp_status gp_ctx_trim(gp_ctx* ctx);
+/* Counters of the context's caching allocator since its creation: blocks
+ * requested, blocks obtained from the driver (cudaMalloc), cached blocks
+ * returned to the driver to make room, and host milliseconds spent in the
+ * allocator.  A partition of a graph seen before normally needs no driver
+ * allocation at all. */
+gp_status gp_ctx_allocator_stats(gp_ctx* ctx, uint64_t* requests, uint64_t* driver_allocs, uint64_t* cache_frees,
+                                 double* host_ms);
 
 /* One SCLP aggregation (replaces gpart::aggregate, include/coarsen.hpp:88-92;
  * src/coarsen.cu:1661-1671).  map: n int32 (host).  cluster_size_factor and

@@ -139,6 +139,26 @@ def test_contraction_large_id_range(ctx):
     assert sizes.max() > 4096
 
 
+def test_contraction_wide_id_range_sorted_rows(ctx):
+    """Coarse ids over more than four bitmap windows (2.6 M): the rows of
+    4,097-65,536 entries are sorted in global memory by one block each
+    instead of the bitmap windows; rows of every other class around them."""
+    off, idx, g = file_graph("rmat22")
+    n = len(off) - 1
+    keep = 2_600_000
+    mapping = np.arange(n, dtype=np.int64)
+    rest = np.arange(keep, n)
+    mapping[keep:] = np.where(rest % 5 == 0, keep + rest % 8, keep + 8 + rest % 2000)
+    mapping = mapping.astype(np.int32)
+    groups = keep + 2008
+    coff, cnbr, cew, cvw = ctx.contract(g, mapping, groups)
+    o = O.contract(O.Graph(off, idx), mapping, groups)
+    assert np.array_equal(coff, o.off) and np.array_equal(cnbr, o.nbr) and np.array_equal(cew, o.ew)
+    assert np.array_equal(cvw, o.vw)
+    scattered = np.bincount(mapping[np.repeat(np.arange(n), np.diff(off))], minlength=groups)
+    assert ((scattered > 4096) & (scattered <= 65536)).sum() >= 1000
+
+
 # --- FP32 diffusion vs FP64 oracle (src/initial_partition_gpu.cu:81-142)
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
