@@ -97,7 +97,7 @@ class RefineStats(ctypes.Structure):
 EXPORTS = ["gp_options_default", "gp_ctx_create", "gp_ctx_destroy", "gp_ctx_error", "gp_partition_capacity",
            "gp_partition", "gp_aggregate", "gp_contract", "gp_coarsen", "gp_hierarchy_levels", "gp_hierarchy_level",
            "gp_hierarchy_write", "gp_hierarchy_free", "gp_initial_partition", "gp_diffusion", "gp_refine", "gp_cut",
-           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_set_hub_tables", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
+           "gp_launch_count", "gp_sync_count", "gp_ctx_set_sync_mode", "gp_ctx_set_device_share", "gp_ctx_set_small_diffusion", "gp_ctx_set_hub_tables", "gp_ctx_set_graph_loops", "gp_ctx_stream", "gp_profile_enable", "gp_profile_dump",
            "gp_initial_partition_static", "gp_initial_partition_trace", "gp_analyze", "gp_symmetrize", "gp_generate_rmat", "gp_partition_range", "gp_ctx_memory", "gp_ctx_trim", "gp_ctx_allocator_stats",
            "gp_footprint_bytes", "gp_server_create", "gp_server_destroy", "gp_server_error", "gp_server_submit",
            "gp_server_submit_range", "gp_server_poll", "gp_server_wait", "gp_partition_batch"]
@@ -144,6 +144,7 @@ def lib() -> ctypes.CDLL:
         L.gp_ctx_set_device_share.argtypes = [vp, i32]
         L.gp_ctx_set_small_diffusion.argtypes = [vp, i32]
         L.gp_ctx_set_hub_tables.argtypes = [vp, i32]
+        L.gp_ctx_set_graph_loops.argtypes = [vp, i32]
         L.gp_ctx_stream.argtypes = [vp]
         L.gp_ctx_stream.restype = vp
         L.gp_profile_enable.argtypes = [vp, i32]
@@ -406,6 +407,11 @@ class Context:
     def set_hub_tables(self, on_chip: bool):
         """On-chip hub hash tables where they fit (same hierarchy)."""
         self._check(lib().gp_ctx_set_hub_tables(self._h, int(on_chip)))
+
+    def set_graph_loops(self, mode: int):
+        """Rebalance loop of the default mode as a CUDA graph: 0 never (host
+        loop, the default), 1 once a level's host loop ran 8 iterations, 2 always."""
+        self._check(lib().gp_ctx_set_graph_loops(self._h, int(mode)))
 
     def set_device_share(self, share: int):
         """Contexts expected to run at once on the device (grid sizing only)."""

@@ -92,6 +92,10 @@ struct Device {
     // SCLP affinity of hubs with on-chip tables where they fit (same
     // results as the global tables); off only to compare the two.
     bool hub_chip = true;
+    // The default mode's rebalance loop as a CUDA graph with a device-side
+    // loop condition: 0 never (host loop, same kernels; the default), 1 once
+    // a level's host loop has run a few iterations, 2 always.
+    int graph_loops = 0;
     int grid_limit(int per_sm) const { return std::max(sms / 2, sms * per_sm / std::max(1, share)); }
     u32* err = nullptr;         // device error word
     void* pinned = nullptr;     // small pinned host staging area

@@ -1295,6 +1295,62 @@ u64 undirected_cut(Device& d, const DGraph<T>& g, const i32* labels, u64* scratc
     return c / 2;
 }
 
+// The rebalance loop on the device (refine_incremental.cuh:303-330 runs it
+// from the host, one round trip per iteration): a CUDA graph holds one
+// conditional WHILE node whose body is the iteration's launches followed by
+// rebalance_continue_kernel, which sums the iteration's counters here and
+// sets the node's condition.
+struct RebalanceLoop {
+    long long delta;   // summed cut decrease of the iterations
+    i64 accepted;      // summed movers
+    int iterations;
+    int stalled;       // the last iteration moved nothing
+};
+
+// One warp, after every iteration: continue while the iteration moved
+// vertices, a part is above capacity and fewer than `limit` iterations ran
+// (the host loop's conditions, so the loop ends after at most `limit`
+// iterations whatever the data).
+__global__ void rebalance_continue_kernel(cudaGraphConditionalHandle handle, const RefineCounters* ctr,
+                                          const u64* pw, int k, u64 cap, int limit, RebalanceLoop* s) {
+    const int lane = threadIdx.x & 31;
+    u64 x = lane < k ? pw[lane] : 0;
+    for (int o = 16; o; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (threadIdx.x != 0) return;
+    const i64 moved = ctr->movers;
+    const int it = ++s->iterations;
+    s->delta += ctr->delta;
+    s->accepted += moved;
+    if (moved == 0) s->stalled = 1;
+    cudaGraphSetConditional(handle, moved != 0 && x > cap && it < limit ? 1u : 0u);
+}
+
+// Rebalance iterations a level runs from the host before the adaptive mode
+// captures its loop into a graph.
+constexpr int kGraphLoopAfter = 8;
+
+// The graph of one level's rebalance loop (its kernels' arguments are the
+// level's buffers, so it is built once per level and launched after every
+// LP round that leaves a part overloaded).
+struct RebalanceGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t capturing = nullptr;   // set while the body is being captured
+    u64 body_launches = 0;              // kernels per iteration
+    RebalanceGraph() = default;
+    RebalanceGraph(const RebalanceGraph&) = delete;
+    RebalanceGraph& operator=(const RebalanceGraph&) = delete;
+    ~RebalanceGraph() {
+        if (capturing) {   // an exception left the capture open: close it, keep nothing
+            cudaGraph_t body = nullptr;
+            cudaStreamEndCapture(capturing, &body);
+            cudaGetLastError();
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
 struct RefineWork {
     Buf<unsigned char> cache_raw;
     Buf<i32> targets, list, movers, saved_labels, clist, clist_alt, cand;
@@ -1422,16 +1478,9 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
     // rebalance apply needs no round trip before its launch: its grids are
     // sized for an upper bound of its movers.
     i64 ncand = 0;   // rebalance candidates in w.cand (vertices of overloaded parts, ascending)
-    auto finish_apply = [&](bool lp) -> i64 {
-        RefineCounters c0{};
-        const bool read_first = lp || d.prof || trace().on;
-        if (read_first) {
-            fetch(d, &c0, ctr, 1);
-            if (c0.movers == 0) return 0;
-        }
-        const i64 bound = read_first ? c0.movers : ncand;
-        const bool rebuild = lp && c0.mover_degree > g.m / 8;
-        trace().mark(d, lp ? "refine.select_lp" : "refine.select_balance", n);
+    // the apply and commit launches for at most `bound` movers (the kernels
+    // read the count from ctr)
+    auto apply_launches = [&](bool lp, i64 bound, bool rebuild) {
         if (!rebuild) {
             // w.list (the LP proposers) is free once the movers are selected:
             // it takes the movers of degree above kSplitDegree
@@ -1450,6 +1499,27 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         launch(d, "commit_kernel", commit_kernel<W>, stride_grid(d, bound), kThreads, 0, w.movers.get(), ctr, labels,
                w.targets.get(), vw, pw, w.locks.get(), w.flags.get(), lp ? 1 : 0);
         if (rebuild) build_cache();
+    };
+    // the cut after a decrease of `delta` (a negative delta raises it)
+    auto apply_delta = [&](long long delta) {
+        if (delta >= 0) {
+            if (static_cast<u64>(delta) > current_cut) fail(GP_ERUNTIME, "incremental cut underflow");
+            current_cut -= static_cast<u64>(delta);
+        } else {
+            current_cut += static_cast<u64>(-delta);
+        }
+    };
+    auto finish_apply = [&](bool lp) -> i64 {
+        RefineCounters c0{};
+        const bool read_first = lp || d.prof || trace().on;
+        if (read_first) {
+            fetch(d, &c0, ctr, 1);
+            if (c0.movers == 0) return 0;
+        }
+        const i64 bound = read_first ? c0.movers : ncand;
+        const bool rebuild = lp && c0.mover_degree > g.m / 8;
+        trace().mark(d, lp ? "refine.select_lp" : "refine.select_balance", n);
+        apply_launches(lp, bound, rebuild);
         trace().mark(d, rebuild ? "refine.rebuild" : "refine.apply", c0.movers, c0.mover_degree);
         // counters and part weights straight into the pinned staging buffer,
         // one wait for both
@@ -1477,17 +1547,8 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
                                                      static_cast<double>(h.c.hub_chunks) * 8 +
                                                      static_cast<double>(h.c.hub_edges) * per_edge);
         }
-        if (rebuild) {
-            current_cut = undirected_cut(d, g, labels, w.scratch.get());
-        } else {
-            const long long delta = h.c.delta;
-            if (delta >= 0) {
-                if (static_cast<u64>(delta) > current_cut) fail(GP_ERUNTIME, "incremental cut underflow");
-                current_cut -= static_cast<u64>(delta);
-            } else {
-                current_cut += static_cast<u64>(-delta);
-            }
-        }
+        if (rebuild) current_cut = undirected_cut(d, g, labels, w.scratch.get());
+        else apply_delta(h.c.delta);
         std::copy(h.pw, h.pw + k, host_pw.begin());
         st.accepted += static_cast<u64>(h.c.movers);
         if (verify) {
@@ -1523,6 +1584,70 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
             count, w.clist.get(), w.bucket.get(), w.excl.get(), w.bucket_base.get(), vw, w.rank.get(), w.counts.get());
         GP_LAUNCH();
     };
+    // The rebalance loop as one graph launch: the iterations' launches are
+    // captured once per level into the body of a WHILE node, and
+    // rebalance_continue_kernel decides on the device whether another
+    // iteration runs.  One round trip at the end reads the summed counters
+    // and the part weights.
+    RebalanceGraph rgraph;
+    Buf<RebalanceLoop> loop_state;
+    int host_iterations = 0;   // rebalance iterations of this level run by the host loop
+    auto rebalance_on_device = [&](const auto& select, int limit) -> bool {
+        if (!rgraph.exec) {
+            loop_state = Buf<RebalanceLoop>(d, 1);
+            GP_CUDA(cudaGraphCreate(&rgraph.graph, 0));
+            cudaGraphConditionalHandle handle = 0;
+            GP_CUDA(cudaGraphConditionalHandleCreate(&handle, rgraph.graph, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams p{};
+            p.type = cudaGraphNodeTypeConditional;
+            p.conditional.handle = handle;
+            p.conditional.type = cudaGraphCondTypeWhile;
+            p.conditional.size = 1;
+            cudaGraphNode_t node = nullptr;
+            GP_CUDA(cudaGraphAddNode(&node, rgraph.graph, nullptr, 0, &p));
+            // thread-local capture: other threads (a server's slots) keep
+            // allocating while this one captures
+            GP_CUDA(cudaStreamBeginCaptureToGraph(d.stream, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+            rgraph.capturing = d.stream;
+            const u64 before = d.launches;
+            select();
+            apply_launches(false, ncand, false);
+            launch(d, "rebalance_continue_kernel", rebalance_continue_kernel, 1, 32, 0, handle, ctr, pw, k, cap, limit,
+                   loop_state.get());
+            rgraph.body_launches = d.launches - before;
+            d.launches = before;
+            cudaGraph_t body = nullptr;
+            rgraph.capturing = nullptr;
+            GP_CUDA(cudaStreamEndCapture(d.stream, &body));
+            GP_CUDA(cudaGraphInstantiate(&rgraph.exec, rgraph.graph, 0));
+        }
+        GP_CUDA(cudaMemsetAsync(loop_state.get(), 0, sizeof(RebalanceLoop), d.stream));
+        GP_CUDA(cudaGraphLaunch(rgraph.exec, d.stream));
+        struct LoopStats { RebalanceLoop s; u64 pw[32]; };
+        static_assert(sizeof(LoopStats) <= Device::kPinnedBytes, "loop stats fit the pinned staging buffer");
+        LoopStats h;
+        {
+            auto* staged = reinterpret_cast<LoopStats*>(d.pinned);
+            GP_CUDA(cudaMemcpyAsync(&staged->s, loop_state.get(), sizeof(RebalanceLoop), cudaMemcpyDeviceToHost,
+                                    d.stream));
+            GP_CUDA(cudaMemcpyAsync(staged->pw, pw, k * sizeof(u64), cudaMemcpyDeviceToHost, d.stream));
+            d.sync();
+            std::memcpy(&h, staged, sizeof(LoopStats));
+        }
+        if (h.s.iterations < 1 || h.s.iterations > limit) fail(GP_ERUNTIME, "rebalance graph iteration count");
+        d.launches += static_cast<u64>(h.s.iterations) * rgraph.body_launches;
+        st.admission_iterations += h.s.iterations;
+        st.accepted += static_cast<u64>(h.s.accepted);
+        apply_delta(h.s.delta);
+        std::copy(h.pw, h.pw + k, host_pw.begin());
+        if (verify) {
+            const u64 recount = undirected_cut(d, g, labels, w.scratch.get());
+            if (recount != current_cut) fail(GP_ERUNTIME, "incremental cut differs from CSR scan");
+        }
+        if (h.s.stalled) return false;
+        return maximum() <= cap;
+    };
     auto rebalance = [&]() -> bool {
         if (maximum() <= cap) return true;
         i64* cand_count = reinterpret_cast<i64*>(w.scratch.get() + 6);
@@ -1538,8 +1663,8 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
         const i64* dev_count = host_count ? nullptr : cand_count;
         const int cgrid = host_count ? blocks_for(std::max<i64>(ncand, 1), kThreads) : stride_grid(d, n);
         w.counts.zero(d);   // bucket_scan_kernel leaves the counts zero for the next pass
-        for (int it = 0; it < 2 * k + 4 && maximum() > cap; ++it) {
-            ++st.admission_iterations;
+        // one iteration's launches up to the movers (refine_incremental.cuh:303-326)
+        auto select = [&]() {
             GP_CUDA(cudaMemsetAsync(ctr, 0, sizeof(RefineCounters), d.stream));
             launch(d, "rebalance_proposals_kernel", rebalance_proposals_kernel<C, W>, cgrid, kThreads, 0, ncand,
                    dev_count, w.cand.get(), cache, labels, vw, k, pw, cap, thresholds.t, deterministic ? 1 : 0, w.targets.get(),
@@ -1558,6 +1683,18 @@ gp_refine_stats refine_level(Device& d, const DGraph<T>& g, RefineWork& w, i32* 
                    dev_count, w.cand.get(), w.bucket.get(), w.rank.get(), w.offsets.get(), pw, cap, vw, w.flags.get(),
                    w.movers.get(), ctr);
             GP_LAUNCH();
+        };
+        const int limit = 2 * k + 4;
+        // Building the graph costs a few hundred microseconds per level, about
+        // the host round trips of ten iterations: mode 1 captures once this
+        // level's host loop has run kGraphLoopAfter iterations, mode 2 at once.
+        if (!host_count && (d.graph_loops == 2 || (d.graph_loops == 1 && (rgraph.exec ||
+                                                                           host_iterations >= kGraphLoopAfter))))
+            return rebalance_on_device(select, limit);
+        for (int it = 0; it < limit && maximum() > cap; ++it) {
+            ++st.admission_iterations;
+            ++host_iterations;
+            select();
             const i64 moved = finish_apply(false);
             if (!moved) return false;
         }
@@ -2331,6 +2468,12 @@ gp_status gp_ctx_set_small_diffusion(gp_ctx* ctx, int enable) {
 gp_status gp_ctx_set_hub_tables(gp_ctx* ctx, int on_chip) {
     if (!ctx) return GP_EINVAL;
     ctx->dev.hub_chip = on_chip != 0;
+    return GP_OK;
+}
+
+gp_status gp_ctx_set_graph_loops(gp_ctx* ctx, int mode) {
+    if (!ctx || mode < 0 || mode > 2) return GP_EINVAL;
+    ctx->dev.graph_loops = mode;
     return GP_OK;
 }
 

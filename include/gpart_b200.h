@@ -314,6 +314,22 @@ gp_status gp_ctx_set_small_diffusion(gp_ctx* ctx, int enable);
  * give the same hierarchy. */
 gp_status gp_ctx_set_hub_tables(gp_ctx* ctx, int on_chip);
 
+/* The rebalance loop of the default (non-deterministic) refinement
+ * (src/refine_incremental.cuh:303-330, one host round trip per iteration in
+ * the reference) as a CUDA graph: the iteration's kernels form the body of a
+ * conditional WHILE node, and a one-warp kernel after them ends the loop on
+ * the device (no mover, no part above capacity, or 2k + 4 iterations); one
+ * round trip per rebalance reads the summed counters.  mode 0 (default)
+ * drives the same kernels from the host; 1 builds a level's graph once that
+ * level's host loop has run 8 iterations (building costs about as much as ten
+ * round trips); 2 uses the graph from a level's first rebalance.  Measured on
+ * one B200 the graph saves host round trips but not consistently time: RMAT-20
+ * partitions ran 3-8% faster, RMAT-24 within run-to-run noise, graphs of
+ * 10^4-10^5 vertices 4-6% slower (their rebalances end after one or two
+ * iterations, so building the graph does not pay).  The deterministic mode
+ * and profiling always use the host loop. */
+gp_status gp_ctx_set_graph_loops(gp_ctx* ctx, int mode);
+
 /* Spectral initial partition that allocates no device memory.
  *
  * For callers that cannot call cudaMalloc: a process whose device memory is
