@@ -393,8 +393,21 @@ __global__ void __launch_bounds__(kThreads) hub_cut_kernel(const Chunk* __restri
     const Chunk ch = chunks[blockIdx.x];
     const i32 s = labels[ch.v];
     u64 local = 0;
-    for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads)
-        if (labels[nbr[e]] != s) local += static_cast<u64>(weight_at(ew, e));
+    // four edges per thread and step: their neighbour ids, then their labels
+    for (i64 e0 = ch.begin + threadIdx.x; e0 < ch.end; e0 += 4 * kThreads) {
+        i32 u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const i64 e = e0 + j * kThreads;
+            u[j] = e < ch.end ? nbr[e] : -1;
+        }
+        i32 lu[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) lu[j] = u[j] >= 0 ? labels[u[j]] : s;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (lu[j] != s) local += static_cast<u64>(weight_at(ew, e0 + j * kThreads));
+    }
     local = block_sum(local, sh);
     if (threadIdx.x == 0 && local) atomic_add_u64(out, local);
 }
@@ -419,18 +432,26 @@ __global__ void __launch_bounds__(kThreads) hub_build_cache_kernel(const Chunk* 
     const i64 len = ch.end - ch.begin;
     const i64 per = (len + kWarps - 1) / kWarps;
     const i64 lo = ch.begin + warp * per, hi = lo + per < ch.end ? lo + per : ch.end;
-    for (i64 base = lo; base < hi; base += 32) {
-        const i64 e = base + lane;
-        int p = -1;
-        u64 w = 0;
-        if (e < hi) {
-            const i32 u = nbr[e];
-            if (u != ch.v) { p = labels[u]; w = static_cast<u64>(weight_at(ew, e)); }
+    // four 32-edge steps at a time: their neighbour ids, then their labels,
+    // then the warp's match and row updates
+    for (i64 base = lo; base < hi; base += 4 * 32) {
+        i32 u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const i64 e = base + j * 32 + lane;
+            u[j] = e < hi ? nbr[e] : ch.v;
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, p);
-        const u64 sum = group_sum<C>(peers, w);
-        if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][p] += sum;
-        __syncwarp();
+        int p[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p[j] = u[j] != ch.v ? labels[u[j]] : -1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u64 w = p[j] >= 0 ? static_cast<u64>(weight_at(ew, base + j * 32 + lane)) : 0;
+            const unsigned peers = __match_any_sync(0xffffffffu, p[j]);
+            const u64 sum = group_sum<C>(peers, w);
+            if (p[j] >= 0 && lane == __ffs(peers) - 1) rows[warp][p[j]] += sum;
+            __syncwarp();
+        }
     }
     __syncthreads();
     if (threadIdx.x < k) {
@@ -519,20 +540,8 @@ __global__ void __launch_bounds__(kThreads) hub_apply_kernel(i64 nchunks, const 
                 atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->hub_edges),
                           static_cast<unsigned long long>(ch.end - ch.begin));
             const i32 v = ch.v;
-            const i32 s = labels[v], t = targets[v];
-            for (i64 e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
-                const i32 u = nbr[e];
-                if (u == v) continue;
-                const u64 w = static_cast<u64>(weight_at(ew, e));
-                cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
-                cache_add(&cache[static_cast<i64>(u) * k + t], w);
-                const bool fu = flags[u] != 0;
-                if (!fu || u > v) {
-                    const i32 lu = labels[u];
-                    const i32 nn = fu ? targets[u] : lu;
-                    gain += static_cast<long long>(w) * ((s != lu) - (t != nn));
-                }
-            }
+            gain += apply_edges_batched(v, labels[v], targets[v], ch.begin, ch.end, static_cast<int>(threadIdx.x),
+                                        kThreads, nbr, ew, labels, targets, flags, k, cache);
         }
         __syncthreads();
     }

@@ -314,25 +314,117 @@ __global__ void __launch_bounds__(kThreads) priority_filter_kernel(
     }
 }
 
-// incremental_update_cache_and_cut (src/refine_incremental.cuh:69-95).  One
-// edge of mover v (label s, target t): the neighbour's cache row loses w at s
-// and gains it at t; the cut change is counted once per undirected edge (the
-// neighbour is not a mover, or has the larger id).
+// incremental_update_cache_and_cut (src/refine_incremental.cuh:69-95) for
+// one edge of mover v (label s, target t): the neighbour's cache row loses w
+// at s and gains it at t; the cut change is counted once per undirected edge
+// (the neighbour is not a mover, or has the larger id).
+//
+// Here over the edges [b, e1) of mover v, thread `tid` of `nthreads`
+// taking every nthreads-th edge, kApplyBatch of them per step: the batch's
+// neighbour ids are loaded first, then their flags and labels, then the cache
+// updates issued, so a thread keeps kApplyBatch independent gather chains in
+// flight instead of one.  Integer sums, so the result does not depend on the
+// order.
+constexpr int kApplyBatch = 4;
+
 template <typename W, typename C>
-__device__ __forceinline__ long long apply_edge(i32 v, i32 s, i32 t, i64 e, const i32* __restrict__ nbr,
-                                                const W* __restrict__ ew, const i32* __restrict__ labels,
-                                                const i32* __restrict__ targets,
-                                                const unsigned char* __restrict__ flags, int k, C* cache) {
-    const i32 u = nbr[e];
-    if (u == v) return 0;
-    const u64 w = static_cast<u64>(weight_at(ew, e));
-    const bool fu = flags[u] != 0;
-    const i32 lu = labels[u];
-    cache_add(&cache[static_cast<i64>(u) * k + s], 0ULL - w);
-    cache_add(&cache[static_cast<i64>(u) * k + t], w);
-    if (fu && u < v) return 0;
-    const i32 nn = fu ? targets[u] : lu;
-    return static_cast<long long>(w) * ((s != lu) - (t != nn));
+__device__ __forceinline__ long long apply_edges_batched(i32 v, i32 s, i32 t, i64 b, i64 e1, int tid, int nthreads,
+                                                         const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                         const i32* __restrict__ labels,
+                                                         const i32* __restrict__ targets,
+                                                         const unsigned char* __restrict__ flags, int k, C* cache) {
+    long long gain = 0;
+    const i64 step = static_cast<i64>(nthreads);
+    for (i64 e0 = b + tid; e0 < e1; e0 += kApplyBatch * step) {
+        i32 u[kApplyBatch];
+#pragma unroll
+        for (int j = 0; j < kApplyBatch; ++j) {
+            const i64 e = e0 + j * step;
+            u[j] = e < e1 ? nbr[e] : v;   // past the row: treated as a self loop, skipped
+        }
+        bool fu[kApplyBatch];
+        i32 lu[kApplyBatch];
+#pragma unroll
+        for (int j = 0; j < kApplyBatch; ++j) {
+            fu[j] = false;
+            lu[j] = 0;
+            if (u[j] != v) {
+                fu[j] = flags[u[j]] != 0;
+                lu[j] = labels[u[j]];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kApplyBatch; ++j) {
+            if (u[j] == v) continue;
+            const u64 w = static_cast<u64>(weight_at(ew, e0 + j * step));
+            cache_add(&cache[static_cast<i64>(u[j]) * k + s], 0ULL - w);
+            cache_add(&cache[static_cast<i64>(u[j]) * k + t], w);
+            if (fu[j] && u[j] < v) continue;
+            const i32 nn = fu[j] ? targets[u[j]] : lu[j];
+            gain += static_cast<long long>(w) * ((s != lu[j]) - (t != nn));
+        }
+    }
+    return gain;
+}
+
+// The same update over the edges of up to 32 movers, one per lane (v, s, t, first
+// edge `begin`, `deg` edges; deg 0 for no mover), walked as warp_edge_walk
+// walks them but kApplyBatch 32-edge steps at a time: each lane resolves its
+// kApplyBatch positions (owning lane, edge) and loads their neighbour ids,
+// then their flags and labels, before any cache update.
+template <typename W, typename C>
+__device__ __forceinline__ long long warp_apply_rows(i32 v, i32 s, i32 t, i64 begin, i64 deg,
+                                                     const i32* __restrict__ nbr, const W* __restrict__ ew,
+                                                     const i32* __restrict__ labels, const i32* __restrict__ targets,
+                                                     const unsigned char* __restrict__ flags, int k, C* cache) {
+    const int lane = threadIdx.x & 31;
+    const i64 inc = warp_inclusive_sum(deg);
+    const i64 pre = inc - deg;
+    const i64 total = __shfl_sync(0xffffffffu, inc, 31);
+    long long gain = 0;
+    for (i64 base = 0; base < total; base += kApplyBatch * 32) {
+        i32 ov[kApplyBatch], os[kApplyBatch], ot[kApplyBatch], u[kApplyBatch];
+        i64 e[kApplyBatch];
+#pragma unroll
+        for (int j = 0; j < kApplyBatch; ++j) {
+            const i64 q = base + j * 32 + lane;
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const i64 probe = __shfl_sync(0xffffffffu, pre, lo + step);
+                if (probe <= q) lo += step;
+            }
+            const i64 my_pre = __shfl_sync(0xffffffffu, pre, lo);
+            const i64 my_begin = __shfl_sync(0xffffffffu, begin, lo);
+            ov[j] = __shfl_sync(0xffffffffu, v, lo);
+            os[j] = __shfl_sync(0xffffffffu, s, lo);
+            ot[j] = __shfl_sync(0xffffffffu, t, lo);
+            e[j] = my_begin + (q - my_pre);
+            u[j] = q < total ? nbr[e[j]] : ov[j];   // past the last edge: treated as a self loop, skipped
+        }
+        bool fu[kApplyBatch];
+        i32 lu[kApplyBatch];
+#pragma unroll
+        for (int j = 0; j < kApplyBatch; ++j) {
+            fu[j] = false;
+            lu[j] = 0;
+            if (u[j] != ov[j]) {
+                fu[j] = flags[u[j]] != 0;
+                lu[j] = labels[u[j]];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kApplyBatch; ++j) {
+            if (u[j] == ov[j]) continue;
+            const u64 w = static_cast<u64>(weight_at(ew, e[j]));
+            cache_add(&cache[static_cast<i64>(u[j]) * k + os[j]], 0ULL - w);
+            cache_add(&cache[static_cast<i64>(u[j]) * k + ot[j]], w);
+            if (fu[j] && u[j] < ov[j]) continue;
+            const i32 nn = fu[j] ? targets[u[j]] : lu[j];
+            gain += static_cast<long long>(w) * ((os[j] != lu[j]) - (ot[j] != nn));
+        }
+    }
+    return gain;
 }
 
 // Movers of degree above this are walked by a whole block
@@ -372,12 +464,7 @@ __global__ void __launch_bounds__(kThreads) apply_cache_cut_kernel(
         if (lane == 0 && walked)
             atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->walked_degree), static_cast<unsigned long long>(walked));
         const i32 s = has ? labels[v] : 0, t = has ? targets[v] : 0;
-        warp_edge_walk(b, deg, [&](bool valid, int owner, i64 e) {
-            const i32 ov = __shfl_sync(0xffffffffu, v, owner);
-            const i32 os = __shfl_sync(0xffffffffu, s, owner);
-            const i32 ot = __shfl_sync(0xffffffffu, t, owner);
-            if (valid) gain += apply_edge(ov, os, ot, e, nbr, ew, labels, targets, flags, k, cache);
-        });
+        gain += warp_apply_rows(v, s, t, b, deg, nbr, ew, labels, targets, flags, k, cache);
     }
     gain = warp_sum(gain);
     if (lane == 0 && gain) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->delta), static_cast<unsigned long long>(gain));
@@ -396,9 +483,9 @@ __global__ void __launch_bounds__(kThreads) apply_big_rows_kernel(
     for (i64 r = blockIdx.x; r < count; r += gridDim.x) {
         const i32 v = big[r];
         const i32 s = labels[v], t = targets[v];
-        const i64 e1 = static_cast<i64>(off[v + 1]);
-        for (i64 e = static_cast<i64>(off[v]) + threadIdx.x; e < e1; e += kThreads)
-            gain += apply_edge(v, s, t, e, nbr, ew, labels, targets, flags, k, cache);
+        gain += apply_edges_batched(v, s, t, static_cast<i64>(off[v]), static_cast<i64>(off[v + 1]),
+                                    static_cast<int>(threadIdx.x), kThreads, nbr, ew, labels, targets, flags, k,
+                                    cache);
     }
     gain = block_sum(gain, sh);
     if (threadIdx.x == 0 && gain)
