@@ -1,4 +1,4 @@
-"""Host-side logic that needs no GPU: the bench's roofline arithmetic."""
+"""Host-side logic that needs no GPU: the bench's roofline arithmetic and its workloads."""
 import sys
 from pathlib import Path
 
@@ -16,3 +16,13 @@ def test_roofline_picks_the_top_modelled_kernel():
     assert r["algorithmic_bytes_per_launch"] == 1e9
     assert r["traffic"] == round(bench.DRAM_PER_ALGORITHMIC_BYTE["hub_insert_kernel"] * 1e9)
     assert abs(r["share_of_gpu_time"] - 2.0 / 8.0) < 1e-9
+
+
+def test_secondary_configs_are_known_workloads():
+    """Both arms measure the same secondary workloads (the configured 320^3
+    grid, big width, k=8 and k=32) after the main one."""
+    import bench
+    assert bench.OTHER_CONFIGS == ("grid3d_320_k8", "grid3d_320_k32")
+    for name in bench.OTHER_CONFIGS:
+        graph, parts, width, _ = bench.WORKLOADS[name]
+        assert graph == "grid3d_320" and width == "big" and parts in (8, 32)
