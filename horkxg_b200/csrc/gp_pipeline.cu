@@ -502,16 +502,19 @@ void aggregate(Device& d, const DGraph<T>& g, SclpWork<T>& w, int parts, u32 see
                    cw, p, so);
         }
         if (direct) return;
+        // 8-byte table slots where every connection sum fits 32 bits
         if (cnt[3])
-            launch(d, "affinity_warp_hash_kernel", affinity_warp_hash_kernel<O, W>, blocks_for(cnt[3], kWarps), kThreads, 0, 
-                cnt[3], class_list(3), off, nbr, ew, vw, clusters, cw, p, so, d.err);
-        if (cnt[4])
-            GP_CUDA(cudaFuncSetAttribute(affinity_block_hash_kernel<O, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kLargeSlots * 12));
-
-        if (cnt[4])
-            launch(d, "affinity_block_hash_kernel", affinity_block_hash_kernel<O, W>, static_cast<int>(cnt[4]), kThreads, kLargeSlots * 12, 
-                cnt[4], class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
+            launch(d, "affinity_warp_hash_kernel",
+                   sum32 ? affinity_warp_hash_kernel<true, O, W> : affinity_warp_hash_kernel<false, O, W>,
+                   blocks_for(cnt[3], kWarps), kThreads, 0, cnt[3], class_list(3), off, nbr, ew, vw, clusters, cw, p,
+                   so, d.err);
+        if (cnt[4]) {
+            auto kernel = sum32 ? affinity_block_hash_kernel<true, O, W> : affinity_block_hash_kernel<false, O, W>;
+            const int smem = kLargeSlots * (sum32 ? 8 : 12);
+            GP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            launch(d, "affinity_block_hash_kernel", kernel, static_cast<int>(cnt[4]), kThreads, smem, cnt[4],
+                   class_list(4), off, nbr, ew, vw, clusters, cw, p, so, d.err);
+        }
         if (cnt[5] && chip) {
             // per processed on-chip hub: its offsets, cluster and proposal
             // writes; per edge its neighbour, weight and cluster gather

@@ -184,6 +184,29 @@ __device__ __forceinline__ void table_insert(i32* keys, u64* vals, u32 mask, i32
     set_error(err, kErrTableFull);
 }
 
+// Packed 8-byte slots for levels whose total edge weight fits 32 bits (every
+// connection sum does): cluster + 1 in the low half (0 = empty), the sum in
+// the high half.  A cluster not yet in the table is claimed together with its
+// first weight by one 64-bit CAS; one already present takes one 32-bit add.
+// Most neighbours of a vertex lie in distinct clusters, so most inserts cost
+// one shared atomic instead of table_insert's two, and a slot takes 8 bytes
+// instead of 12.
+__device__ __forceinline__ void packed_insert(unsigned long long* slots, u32 mask, i32 c, u64 w, u32* err) {
+    const u32 key = static_cast<u32>(c) + 1;
+    const unsigned long long fresh = (static_cast<unsigned long long>(static_cast<u32>(w)) << 32) | key;
+    u32 slot = mix32(static_cast<u32>(c)) & mask;
+    for (u32 probe = 0; probe <= mask; ++probe) {
+        const unsigned long long found = atomicCAS(&slots[slot], 0ULL, fresh);
+        if (found == 0ULL) return;
+        if (static_cast<u32>(found) == key) {
+            atomicAdd(reinterpret_cast<u32*>(&slots[slot]) + 1, static_cast<u32>(w));
+            return;
+        }
+        slot = (slot + 1) & mask;
+    }
+    set_error(err, kErrTableFull);
+}
+
 // Candidate of one table slot.
 __device__ __forceinline__ void slot_candidate(i32 key, u64 conn, u32 v, i32 source, const RoundParams& p,
                                                u64& current, u64& best, u64& tie) {
@@ -199,13 +222,14 @@ __device__ __forceinline__ void slot_candidate(i32 key, u64 conn, u32 v, i32 sou
 
 // Warp per vertex, shared hash of kMediumSlots per warp (cf.
 // sclp_affinity_medium_hash_kernel, :405-476).
-template <typename O, typename W>
+// PACKED: 8-byte slots (packed_insert), for levels with p.sum32.
+template <bool PACKED, typename O, typename W>
 __global__ void __launch_bounds__(kThreads) affinity_warp_hash_kernel(
     i64 count, const i32* __restrict__ list, const O* __restrict__ off, const i32* __restrict__ nbr,
     const W* __restrict__ ew, const W* __restrict__ vw, const i32* __restrict__ clusters,
     const u64* __restrict__ cw, RoundParams p, SclpOut out, u32* err) {
-    __shared__ i32 keys_all[kWarps][kMediumSlots];
-    __shared__ u64 vals_all[kWarps][kMediumSlots];
+    constexpr int kSlotBytes = PACKED ? 8 : 12;
+    __shared__ __align__(16) unsigned char table_all[kWarps][kMediumSlots * kSlotBytes];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 gid = static_cast<i64>(blockIdx.x) * kWarps + warp;
     if (gid >= count) return;
@@ -215,20 +239,33 @@ __global__ void __launch_bounds__(kThreads) affinity_warp_hash_kernel(
         if (lane == 0) out.target[v] = kInvalid;
         return;
     }
-    i32* keys = keys_all[warp];
-    u64* vals = vals_all[warp];
-    for (int s = lane; s < kMediumSlots; s += 32) { keys[s] = -1; vals[s] = 0; }
+    auto* slots = reinterpret_cast<unsigned long long*>(table_all[warp]);   // PACKED
+    u64* vals = reinterpret_cast<u64*>(table_all[warp]);                     // !PACKED
+    i32* keys = reinterpret_cast<i32*>(vals + kMediumSlots);
+    for (int s = lane; s < kMediumSlots; s += 32) {
+        if constexpr (PACKED) { slots[s] = 0ULL; } else { keys[s] = -1; vals[s] = 0; }
+    }
     __syncwarp();
     const i64 begin = off[v], end = off[v + 1];
     for (i64 e = begin + lane; e < end; e += 32) {
         const i32 u = nbr[e];
         if (u == v) continue;
-        table_insert(keys, vals, kMediumSlots - 1, p.identity ? u : clusters[u],
-                     static_cast<u64>(weight_at(ew, e)), err);
+        const i32 c = p.identity ? u : clusters[u];
+        const u64 w = static_cast<u64>(weight_at(ew, e));
+        if constexpr (PACKED) packed_insert(slots, kMediumSlots - 1, c, w, err);
+        else table_insert(keys, vals, kMediumSlots - 1, c, w, err);
     }
     __syncwarp();
     u64 current = 0, best = 0, tie = 0;
-    for (int s = lane; s < kMediumSlots; s += 32) slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
+    for (int s = lane; s < kMediumSlots; s += 32) {
+        if constexpr (PACKED) {
+            const unsigned long long x = slots[s];
+            const u32 key = static_cast<u32>(x);
+            if (key) slot_candidate(static_cast<i32>(key - 1), x >> 32, static_cast<u32>(v), source, p, current, best, tie);
+        } else {
+            slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
+        }
+    }
     group_reduce(current, best, tie, 32, 0xffffffffu);
     if (lane == 0) decode_and_write(v, source, current, best, tie, p, vw, cw, out);
 }
@@ -248,14 +285,16 @@ __device__ __forceinline__ void block_candidate_reduce(u64& current, u64& best, 
     }
 }
 
-// Block per vertex with a kLargeSlots shared hash.
-template <typename O, typename W>
+// Block per vertex with a kLargeSlots shared hash (PACKED: 8-byte slots,
+// for levels with p.sum32; dynamic shared memory kLargeSlots * 8, else * 12).
+template <bool PACKED, typename O, typename W>
 __global__ void __launch_bounds__(kThreads) affinity_block_hash_kernel(
     i64 count, const i32* __restrict__ list, const O* __restrict__ off, const i32* __restrict__ nbr,
     const W* __restrict__ ew, const W* __restrict__ vw, const i32* __restrict__ clusters,
     const u64* __restrict__ cw, RoundParams p, SclpOut out, u32* err) {
     extern __shared__ unsigned char smem_raw[];
-    u64* vals = reinterpret_cast<u64*>(smem_raw);
+    auto* slots = reinterpret_cast<unsigned long long*>(smem_raw);   // PACKED
+    u64* vals = reinterpret_cast<u64*>(smem_raw);                     // !PACKED
     i32* keys = reinterpret_cast<i32*>(vals + kLargeSlots);
     __shared__ CandShared red;
     const i64 gid = blockIdx.x;
@@ -267,19 +306,31 @@ __global__ void __launch_bounds__(kThreads) affinity_block_hash_kernel(
         return;
     }
     const i64 begin = off[v], end = off[v + 1];
-    int slots = 512;   // power of two >= 2 * degree (degree <= kHubDegree)
-    while (slots < 2 * (end - begin) && slots < kLargeSlots) slots <<= 1;
-    for (int s = threadIdx.x; s < slots; s += kThreads) { keys[s] = -1; vals[s] = 0; }
+    int nslots = 512;   // power of two >= 2 * degree (degree <= kHubDegree)
+    while (nslots < 2 * (end - begin) && nslots < kLargeSlots) nslots <<= 1;
+    for (int s = threadIdx.x; s < nslots; s += kThreads) {
+        if constexpr (PACKED) { slots[s] = 0ULL; } else { keys[s] = -1; vals[s] = 0; }
+    }
     __syncthreads();
     for (i64 e = begin + threadIdx.x; e < end; e += kThreads) {
         const i32 u = nbr[e];
         if (u == v) continue;
-        table_insert(keys, vals, static_cast<u32>(slots - 1), p.identity ? u : clusters[u],
-                     static_cast<u64>(weight_at(ew, e)), err);
+        const i32 c = p.identity ? u : clusters[u];
+        const u64 w = static_cast<u64>(weight_at(ew, e));
+        if constexpr (PACKED) packed_insert(slots, static_cast<u32>(nslots - 1), c, w, err);
+        else table_insert(keys, vals, static_cast<u32>(nslots - 1), c, w, err);
     }
     __syncthreads();
     u64 current = 0, best = 0, tie = 0;
-    for (int s = threadIdx.x; s < slots; s += kThreads) slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
+    for (int s = threadIdx.x; s < nslots; s += kThreads) {
+        if constexpr (PACKED) {
+            const unsigned long long x = slots[s];
+            const u32 key = static_cast<u32>(x);
+            if (key) slot_candidate(static_cast<i32>(key - 1), x >> 32, static_cast<u32>(v), source, p, current, best, tie);
+        } else {
+            slot_candidate(keys[s], vals[s], static_cast<u32>(v), source, p, current, best, tie);
+        }
+    }
     block_candidate_reduce(current, best, tie, red);
     if (threadIdx.x == 0) decode_and_write(v, source, current, best, tie, p, vw, cw, out);
 }
