@@ -155,13 +155,36 @@ struct Device {
             if (it->second.empty()) free_blocks.erase(it);
         }
     }
+    // The cached list a request of class c is served from: its own class,
+    // else the smallest larger class within kReuseSlack (a block at most 25%
+    // larger than asked for).  Hierarchies of the same graph at another seed,
+    // or of a graph of similar size, differ by a few percent per buffer;
+    // exact classes alone sent those buffers to the driver, at several
+    // milliseconds per cudaMalloc.  Near the device's capacity (`pressure`:
+    // set once the driver has refused an allocation, or up front for a graph
+    // whose projected footprint exceeds half the device) only exact classes
+    // are reused, so that no live block carries an unused tail there and the
+    // cache keeps the classes the graph asks for (RMAT-26: reusing larger
+    // blocks without bound ran out of memory, and a cache shaped by the slack
+    // before the first refusal thrashed afterwards).
+    static constexpr size_t kReuseSlack = 4;   // c + c / 4
+    bool pressure = false;
+    std::map<size_t, std::vector<void*>>::iterator cached_for(size_t c) {
+        auto it = free_blocks.find(c);
+        if (it != free_blocks.end() && !it->second.empty()) return it;
+        if (pressure) return free_blocks.end();
+        for (it = free_blocks.upper_bound(c); it != free_blocks.end() && it->first <= c + c / kReuseSlack; ++it)
+            if (!it->second.empty()) return it;
+        return free_blocks.end();
+    }
     void* alloc(size_t bytes) {
         if (bytes == 0) return nullptr;
         const auto t0 = std::chrono::steady_clock::now();
-        const size_t c = size_class(bytes);
+        size_t c = size_class(bytes);
         void* p = nullptr;
-        auto it = free_blocks.find(c);
-        if (it != free_blocks.end() && !it->second.empty()) {
+        auto it = cached_for(c);
+        if (it != free_blocks.end()) {
+            c = it->first;   // the block keeps its own class (release files it there)
             p = it->second.back();
             it->second.pop_back();
             cached_bytes -= c;
@@ -169,6 +192,7 @@ struct Device {
             cudaError_t e = driver_alloc(&p, c);
             if (e != cudaSuccess) {   // release part of the cache, then all of it
                 cudaGetLastError();
+                pressure = true;
                 release_cached(c);
                 e = driver_alloc(&p, c);
             }

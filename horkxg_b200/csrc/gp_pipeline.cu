@@ -2516,6 +2516,15 @@ gp_status partition_impl(gp_ctx* ctx, const gp_graph* graph, gp::i64 base, const
             rep.n = graph->n;
             rep.m = graph->m;
             gp::partition_capacity(static_cast<gp::u64>(graph->n), o.parts, o.ratio);
+            if (!d.pressure) {
+                // a graph projected to take more than half the device reuses
+                // cached blocks by exact size class only (Device::cached_for)
+                size_t free_bytes = 0, total_bytes = 0;
+                GP_CUDA(cudaMemGetInfo(&free_bytes, &total_bytes));
+                const gp::u64 fp = gp_footprint_bytes(graph->n, graph->m, o.parts, graph->width,
+                                                      graph->index64 && graph->memory == GP_MEMORY_HOST);
+                if (fp > total_bytes / 2) d.pressure = true;
+            }
             const auto prep_start = gp::Clock::now();
             gp::DGraph<T> g;
             gp::prepare_graph<T>(d, graph, g, o.verify, base);
