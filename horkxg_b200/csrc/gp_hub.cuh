@@ -419,9 +419,11 @@ __global__ void __launch_bounds__(kThreads) hub_build_cache_kernel(const Chunk* 
                                                                    const W* __restrict__ ew,
                                                                    const i32* __restrict__ labels, int k, C* cache) {
     __shared__ u64 rows[kWarps][32];
+    u32 (*rows32)[32] = reinterpret_cast<u32 (*)[32]>(&rows[0][0]);   // C = u32: 32-bit accumulators
     const Chunk ch = chunks[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    rows[warp][lane] = 0;
+    if constexpr (sizeof(C) == 4) rows32[warp][lane] = 0;
+    else rows[warp][lane] = 0;
     __syncwarp();
     // each warp walks its own contiguous slice of the chunk
     const i64 len = ch.end - ch.begin;
@@ -442,16 +444,20 @@ __global__ void __launch_bounds__(kThreads) hub_build_cache_kernel(const Chunk* 
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const u64 w = p[j] >= 0 ? static_cast<u64>(weight_at(ew, base + j * 32 + lane)) : 0;
-            const unsigned peers = __match_any_sync(0xffffffffu, p[j]);
-            const u64 sum = group_sum<C>(peers, w);
-            if (p[j] >= 0 && lane == __ffs(peers) - 1) rows[warp][p[j]] += sum;
+            if constexpr (sizeof(C) == 4) {   // as build_cache_kernel: 32-bit shared atomics
+                if (p[j] >= 0) atomicAdd(&rows32[warp][p[j]], static_cast<u32>(w));
+            } else {
+                const unsigned peers = __match_any_sync(0xffffffffu, p[j]);
+                const u64 sum = group_sum<C>(peers, w);
+                if (p[j] >= 0 && lane == __ffs(peers) - 1) rows[warp][p[j]] += sum;
+            }
             __syncwarp();
         }
     }
     __syncthreads();
     if (threadIdx.x < k) {
         u64 t = 0;
-        for (int w2 = 0; w2 < kWarps; ++w2) t += rows[w2][threadIdx.x];
+        for (int w2 = 0; w2 < kWarps; ++w2) t += sizeof(C) == 4 ? rows32[w2][threadIdx.x] : rows[w2][threadIdx.x];
         if (t) cache_add(&cache[static_cast<i64>(ch.v) * k + threadIdx.x], t);
     }
 }

@@ -138,17 +138,21 @@ __device__ __forceinline__ void load_row(const C* row, int k, C (&vals)[32]) {
 // incremental_build_affinity (src/refine_incremental.cuh:7-25).  A warp
 // takes four consecutive vertices: rows of at most 32 entries are walked by
 // 8 lanes each (up to four steps, all four rows at once), longer rows (up to
-// the hub degree) by the whole warp one after the other.  Lanes holding the
-// same part are grouped with __match_any_sync and only the group leader adds
-// to the row's private accumulator in shared memory, so no atomics are
-// needed; the four cache rows, consecutive in memory, are then stored by the
-// whole warp in one coalesced pass.  Hub rows are left to the chunked kernel
+// the hub degree) by the whole warp one after the other.  Each row is summed
+// in a private accumulator in shared memory: with a 32-bit cache (every sum
+// fits 32 bits) every lane adds its edge with a 32-bit shared atomic; with a
+// 64-bit cache lanes holding the same part are grouped with __match_any_sync
+// and only the group leader adds their sum (measured at RMAT-24: the 32-bit
+// atomics take 26% less time than the match, 64-bit shared atomics 45% more).
+// The four cache rows, consecutive in memory, are then stored by the whole
+// warp in one coalesced pass.  Hub rows are left to the chunked kernel
 // (zero_hub_rows_kernel clears them after this one).
 template <typename O, typename W, typename C>
 __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* __restrict__ off,
                                                                const i32* __restrict__ nbr, const W* __restrict__ ew,
                                                                const i32* __restrict__ labels, int k, C* cache) {
     __shared__ u64 rows[kWarps][4][32];
+    u32 (*rows32)[4][32] = reinterpret_cast<u32 (*)[4][32]>(&rows[0][0][0]);   // C = u32: 32-bit accumulators
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane >> 3, gl = lane & 7;
     const i64 warps_total = static_cast<i64>(gridDim.x) * kWarps;
     for (i64 q = static_cast<i64>(blockIdx.x) * kWarps + warp; q * 4 < n; q += warps_total) {
@@ -159,7 +163,10 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
             deg = static_cast<i64>(off[v + 1]) - b;
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) rows[warp][grp][gl + 8 * j] = 0;
+        for (int j = 0; j < 4; ++j) {
+            if constexpr (sizeof(C) == 4) rows32[warp][grp][gl + 8 * j] = 0;
+            else rows[warp][grp][gl + 8 * j] = 0;
+        }
         __syncwarp();
         const bool short_row = deg <= 32;
         const unsigned steps = __reduce_max_sync(0xffffffffu, short_row ? static_cast<unsigned>((deg + 7) >> 3) : 0u);
@@ -171,9 +178,13 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
                 const i32 u = nbr[b + e];
                 if (u != v) { p = labels[u]; w = static_cast<u64>(weight_at(ew, b + e)); }
             }
-            const unsigned peers = __match_any_sync(0xffffffffu, p < 0 ? -1 - grp : grp * 32 + p);
-            const u64 sum = group_sum<C>(peers, w);
-            if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][grp][p] += sum;
+            if constexpr (sizeof(C) == 4) {
+                if (p >= 0) atomicAdd(&rows32[warp][grp][p], static_cast<u32>(w));
+            } else {
+                const unsigned peers = __match_any_sync(0xffffffffu, p < 0 ? -1 - grp : grp * 32 + p);
+                const u64 sum = group_sum<C>(peers, w);
+                if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][grp][p] += sum;
+            }
             __syncwarp();
         }
         // rows of 33..kHubDegree entries, one at a time by the whole warp
@@ -192,9 +203,13 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
                     const i32 u = nbr[lb + e];
                     if (u != lv) { p = labels[u]; w = static_cast<u64>(weight_at(ew, lb + e)); }
                 }
-                const unsigned peers = __match_any_sync(0xffffffffu, p);
-                const u64 sum = group_sum<C>(peers, w);
-                if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][g][p] += sum;
+                if constexpr (sizeof(C) == 4) {
+                    if (p >= 0) atomicAdd(&rows32[warp][g][p], static_cast<u32>(w));
+                } else {
+                    const unsigned peers = __match_any_sync(0xffffffffu, p);
+                    const u64 sum = group_sum<C>(peers, w);
+                    if (p >= 0 && lane == __ffs(peers) - 1) rows[warp][g][p] += sum;
+                }
                 __syncwarp();
             }
         }
@@ -205,7 +220,10 @@ __global__ void __launch_bounds__(kThreads) build_cache_kernel(i64 n, const O* _
         C* dst = cache + first * k;
         for (int i = lane; i < nrows * k; i += 32) {
             const int row = i / k;
-            if (!(hub_rows & (1u << (row * 8)))) dst[i] = static_cast<C>(rows[warp][row][i - row * k]);
+            if (!(hub_rows & (1u << (row * 8)))) {
+                if constexpr (sizeof(C) == 4) dst[i] = static_cast<C>(rows32[warp][row][i - row * k]);
+                else dst[i] = static_cast<C>(rows[warp][row][i - row * k]);
+            }
         }
         __syncwarp();
     }
