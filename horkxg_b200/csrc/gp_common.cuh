@@ -101,8 +101,13 @@ struct Device {
     void* pinned = nullptr;     // small pinned host staging area
     static constexpr size_t kPinnedBytes = 1 << 16;
 
-    cudaError_t driver_alloc(void** p, size_t bytes) { return cudaMalloc(p, bytes); }
-    void driver_free(void* p) { cudaFree(p); }
+    // The driver calls behind the cache.  A host test replaces them with a
+    // fake device (a byte budget) to exercise the reuse policy and the
+    // out-of-memory path without a GPU.
+    cudaError_t (*malloc_fn)(void**, size_t) = [](void** p, size_t bytes) { return cudaMalloc(p, bytes); };
+    cudaError_t (*free_fn)(void*) = [](void* p) { return cudaFree(p); };
+    cudaError_t driver_alloc(void** p, size_t bytes) { return malloc_fn(p, bytes); }
+    void driver_free(void* p) { free_fn(p); }
 
     std::map<size_t, std::vector<void*>> free_blocks;
     std::unordered_map<void*, size_t> live;

@@ -1,4 +1,5 @@
-"""Host-side logic that needs no GPU: the bench's roofline arithmetic and its workloads."""
+"""Host-side logic that needs no GPU: the bench's roofline arithmetic and workloads, and the
+caching allocator's policy over a fake driver."""
 import sys
 from pathlib import Path
 
@@ -26,3 +27,24 @@ def test_secondary_configs_are_known_workloads():
     for name in bench.OTHER_CONFIGS:
         graph, parts, width, _ = bench.WORKLOADS[name]
         assert graph == "grid3d_320" and width == "big" and parts in (8, 32)
+
+
+def test_allocator_policy_on_a_fake_device(tmp_path):
+    """The caching allocator's reuse rules (exact class, a cached block up to
+    25% larger, exact classes only under memory pressure) and its
+    out-of-memory path (evict the smallest sufficient cached block, retry,
+    else GP_ENOMEM), run by tests/alloc_policy.cu over a fake driver: no GPU."""
+    import shutil
+    import subprocess
+    import pytest
+    root = Path(__file__).resolve().parents[1]
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("nvcc not available")
+    exe = tmp_path / "alloc_policy"
+    subprocess.run([nvcc, "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a", "-I",
+                    str(root / "include"), "-o", str(exe), str(root / "tests" / "alloc_policy.cu")],
+                   check=True, capture_output=True, timeout=600)
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "all checks passed" in run.stdout
