@@ -96,6 +96,7 @@ struct Device {
     // loop condition: 0 never (host loop, same kernels; the default), 1 once
     // a level's host loop has run a few iterations, 2 always.
     int graph_loops = 0;
+    size_t total_bytes = 0;     // device memory, read once when the context is created
     int grid_limit(int per_sm) const { return std::max(sms / 2, sms * per_sm / std::max(1, share)); }
     u32* err = nullptr;         // device error word
     void* pinned = nullptr;     // small pinned host staging area

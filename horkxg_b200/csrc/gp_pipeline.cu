@@ -2425,6 +2425,8 @@ gp_status gp_ctx_create(int device, gp_ctx** out) {
         d.device = device;
         GP_CUDA(cudaSetDevice(device));
         GP_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
+        size_t free_bytes = 0;
+        GP_CUDA(cudaMemGetInfo(&free_bytes, &d.total_bytes));   // once: the query costs milliseconds
         GP_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
         GP_CUDA(cudaMalloc(&d.err, 64));
         GP_CUDA(cudaMemset(d.err, 0, 64));
@@ -2519,11 +2521,9 @@ gp_status partition_impl(gp_ctx* ctx, const gp_graph* graph, gp::i64 base, const
             if (!d.pressure) {
                 // a graph projected to take more than half the device reuses
                 // cached blocks by exact size class only (Device::cached_for)
-                size_t free_bytes = 0, total_bytes = 0;
-                GP_CUDA(cudaMemGetInfo(&free_bytes, &total_bytes));
                 const gp::u64 fp = gp_footprint_bytes(graph->n, graph->m, o.parts, graph->width,
                                                       graph->index64 && graph->memory == GP_MEMORY_HOST);
-                if (fp > total_bytes / 2) d.pressure = true;
+                if (fp > d.total_bytes / 2) d.pressure = true;
             }
             const auto prep_start = gp::Clock::now();
             gp::DGraph<T> g;
