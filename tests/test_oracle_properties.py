@@ -8,7 +8,7 @@ weight is the fine weight between different clusters, its vertex weights are
 the clusters' sums; an aggregation map covers every coarse id and keeps every
 cluster within the returned cap (max(heaviest vertex, average cap), so a
 singleton never exceeds it).  Hypothesis draws the graphs derandomized: the
-same examples every run.
+same examples every run."""
 import numpy as np
 from hypothesis import given, settings, strategies as st
 
