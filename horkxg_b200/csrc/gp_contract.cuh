@@ -314,7 +314,29 @@ __global__ void __launch_bounds__(kThreads) segment_smem_kernel(i64 rows, const 
     const i32 c = list[r];
     const i64 s = temp_off[c];
     const i64 len = temp_off[c + 1] - s;
-    for (i64 i = threadIdx.x; i < len; i += kThreads) { k0[i] = tgt[s + i]; w0[i] = wt[s + i]; }
+    // The row into shared memory with 128-bit loads: entries before the
+    // first 16-byte boundary of the targets (tgt and wt are whole allocator
+    // blocks, so tgt + s is 16-byte aligned when s is a multiple of 4, and wt
+    // + s then too) and after the last whole group of four go by element.
+    const u32* src_k = tgt + s;
+    const W* src_w = wt + s;
+    const i64 head = ((4 - (s & 3)) & 3) < len ? ((4 - (s & 3)) & 3) : len;
+    const i64 groups = (len - head) / 4;
+    for (i64 i = threadIdx.x; i < head; i += kThreads) { k0[i] = src_k[i]; w0[i] = src_w[i]; }
+    for (i64 q = threadIdx.x; q < groups; q += kThreads) {
+        const i64 i = head + 4 * q;
+        const uint4 kk = *reinterpret_cast<const uint4*>(src_k + i);
+        k0[i] = kk.x; k0[i + 1] = kk.y; k0[i + 2] = kk.z; k0[i + 3] = kk.w;
+        if constexpr (sizeof(W) == 4) {
+            const uint4 ww = *reinterpret_cast<const uint4*>(src_w + i);
+            w0[i] = ww.x; w0[i + 1] = ww.y; w0[i + 2] = ww.z; w0[i + 3] = ww.w;
+        } else {
+            const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(src_w + i);
+            const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(src_w + i + 2);
+            w0[i] = a.x; w0[i + 1] = a.y; w0[i + 2] = b.x; w0[i + 3] = b.y;
+        }
+    }
+    for (i64 i = head + 4 * groups + threadIdx.x; i < len; i += kThreads) { k0[i] = src_k[i]; w0[i] = src_w[i]; }
     __syncthreads();
     block_radix_sort_segment(k0, w0, k1, w1, len, 0, key_bits, rank_sh);
     const i64 u = block_reduce_runs(k0, w0, len, sentinel, tgt + s, wt + s, run_sh);
